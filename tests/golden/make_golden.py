@@ -1,0 +1,267 @@
+"""Generate the golden vectors in this folder by executing the reference's own
+source files (``src/initialization.py``, ``src/taichi_variable_definition.py``,
+``src/simulation.py``, ``src/parameter_fitting_functions.py`` of
+denzelzheng/diffcp) unmodified, under the NumPy stand-ins for ``taichi`` and
+``open3d`` in ``ti_standin.py`` / ``o3d_standin.py``.
+
+The reference is copied (read-only sources) into a temporary tree together
+with a small synthetic scene (mesh PLY, grasp trajectory, target clouds, cube
+marker and a ``simulation_arguments.json`` with small sizes), because the
+reference loads its data and configuration from paths relative to itself.
+
+Outputs
+  ref_forward_f32.npz   per-substep states, losses and scene constants of two
+                        grasp windows, reference kernels in float32
+  ref_svd_backward.npz  ``backward_inplane_svd`` (simulation.py:71-88) on
+                        random and degenerate 2x2 inputs
+  ref_fd_f64.npz        central finite differences of the window-0 loss with
+                        respect to E, nu, contact/shearing stiffness and two
+                        grasp-trajectory coordinates, reference kernels in
+                        float64
+
+Run:  python tests/golden/make_golden.py  [--ref PATH]   (needs the reference tree)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import random
+import shutil
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SEED_OP, SEED_CUBE, SEED_SCENE = 1234, 4321, 7
+
+ARGS = {
+    "dt": 0.0002,
+    "n_grid": 15,
+    "scene_scaling": 0.5,
+    "initial_frame": 0,
+    "end_frame": -1,
+    "operator_update_interval": 0.00073,
+    "clip_IFS": 0.8,
+    "grad_update_interval": 0.0061,
+    "operator_parameters": {"operator_edge_length": 0.03, "n_operator_particles": 8, "operator_mass": 99},
+    "rigid_cube_parameters": {"rigid_cube_side_length": 0.14, "n_rigid_cube_particles": 6, "cube_mass": 999},
+    "garment_parameters": {
+        "number_of_triangles": 1500, "sim_number_of_triangles": 310,
+        "constitutive_parameter_upper_bounds": {"E": 1000, "nu": 0.45, "contact_stiffness": 5000,
+                                                "shearing_stiffness": 1000},
+        "constitutive_parameter_lower_bounds": {"E": 10, "nu": 0.05, "contact_stiffness": 10,
+                                                "shearing_stiffness": 1, "internal_friction_angle": 1,
+                                                "damping": 0.1},
+        "initial_constitutive_parameters": {"E": 100, "nu": 0.1, "contact_stiffness": 100,
+                                            "shearing_stiffness": 100},
+        "garment_mass": 0.5},
+    "data_dir": "/../data/",
+    "result_dir": "/../result/",
+    "n_pose_estimation_output": 35,
+}
+PARAMS = {"E": 400.0, "nu": 0.3, "contact_stiffness": 300.0, "shearing_stiffness": 150.0}
+
+
+def write_ply(path, v, t):
+    v = np.asarray(v, dtype="<f8")
+    t = np.asarray(t, dtype="<u4")
+    head = ("ply\nformat binary_little_endian 1.0\ncomment synthetic\nelement vertex %d\n"
+            "property double x\nproperty double y\nproperty double z\nelement face %d\n"
+            "property list uchar uint vertex_indices\nend_header\n" % (len(v), len(t)))
+    rec = np.zeros(len(t), dtype=[("n", "u1"), ("idx", "<u4", (3,))])
+    rec["n"] = 3
+    rec["idx"] = t
+    with open(path, "wb") as fh:
+        fh.write(head.encode("ascii"))
+        fh.write(v.tobytes())
+        fh.write(rec.tobytes())
+
+
+def scene_arrays():
+    """Jittered 7x7 sheet (raw units), a 2-point grasp trajectory moving the two
+    far corners, 2 windows x 12 target points, a cube marker."""
+    rng = np.random.default_rng(SEED_SCENE)
+    n = 7
+    ii, kk = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    verts = np.stack([0.55 + 0.1 * ii, 0.02 + 0.004 * rng.standard_normal((n, n)),
+                      0.30 + 0.1 * kk], -1).reshape(-1, 3)
+    verts[:, [0, 2]] += 0.01 * rng.standard_normal((n * n, 2))
+    tris = []
+    for a in range(n - 1):
+        for b in range(n - 1):
+            v0, v1, v2, v3 = a * n + b, (a + 1) * n + b, a * n + b + 1, (a + 1) * n + b + 1
+            tris.append((v0, v1, v3) if (a + b) % 2 == 0 else (v0, v1, v2))
+            tris.append((v0, v3, v2) if (a + b) % 2 == 0 else (v1, v3, v2))
+    tris = np.array(tris)
+    frames = 20
+    t = np.arange(frames)[:, None]
+    c0 = verts[(n - 1) * n + 0] + np.array([0.0, 0.02, 0.0])
+    c1 = verts[(n - 1) * n + n - 1] + np.array([0.0, 0.02, 0.0])
+    traj = np.stack([c0 + t * np.array([0.012, 0.010, -0.004]),
+                     c1 + t * np.array([0.010, 0.012, 0.006])], 1)
+    traj += 0.001 * rng.standard_normal(traj.shape)
+    target = verts[None, rng.choice(n * n, 12, replace=False)] + 0.02 * rng.standard_normal((2, 12, 3))
+    mark = np.array([0.85, 0.09, 0.55])
+    return verts, tris, traj, target, mark
+
+
+def build_tree(ref):
+    tmp = tempfile.mkdtemp(prefix="diffcp_ref_")
+    os.makedirs(os.path.join(tmp, "src"))
+    os.makedirs(os.path.join(tmp, "data"))
+    os.makedirs(os.path.join(tmp, "result"))
+    for name in os.listdir(os.path.join(ref, "src")):
+        if name.endswith(".py"):
+            shutil.copy(os.path.join(ref, "src", name), os.path.join(tmp, "src", name))
+    open(os.path.join(tmp, "src", "__init__.py"), "w").close()
+    with open(os.path.join(tmp, "src", "simulation_arguments.json"), "w") as fh:
+        json.dump(ARGS, fh)
+    verts, tris, traj, target, mark = scene_arrays()
+    write_ply(os.path.join(tmp, "data", "cloth_mesh.ply"), verts, tris)
+    np.save(os.path.join(tmp, "data", "grasp_traj_array.npy"), traj)
+    np.save(os.path.join(tmp, "data", "target_pcd_sample.npy"), target)
+    np.save(os.path.join(tmp, "data", "rigid_cube_top_face_center_position.npy"), mark)
+    return tmp
+
+
+def import_reference(tree, f64=False):
+    sys.path.insert(0, HERE)
+    import ti_standin
+    import o3d_standin
+    import types
+    if f64:
+        ti_standin.force_f64()
+    sys.modules["taichi"] = ti_standin
+    sys.modules["taichi_glsl"] = types.ModuleType("taichi_glsl")
+    sys.modules["open3d"] = o3d_standin
+    random.seed(SEED_OP)
+    np.random.seed(SEED_CUBE)
+    sys.path.insert(0, tree)
+    import src.parameter_fitting_functions as pff   # noqa: E402  (executes the reference modules)
+    return pff
+
+
+def set_params(m, p):
+    m.garment_E[None] = p["E"]
+    m.garment_nu[None] = p["nu"]
+    m.contact_stiffness[None] = p["contact_stiffness"]
+    m.shearing_stiffness[None] = p["shearing_stiffness"]
+
+
+def window_loss(m, g, keep=False):
+    """The body of compute_grad (parameter_fitting_functions.py:21-29) without
+    the tape: clear, set targets, substeps 0..max_steps-2, compute_loss."""
+    m.initialize_objects()
+    m.clear_distances()
+    m.target_pos.from_numpy(m.target_pcd_array[g])
+    m.loss[None] = 0
+    for f in range(m.max_steps - 1):
+        m.forward(f, g)
+    m.compute_loss(f)
+    return float(m.loss[None])
+
+
+def run_forward32(tree, out):
+    m = import_reference(tree)
+    set_params(m, PARAMS)
+    rec = {}
+    keys = ["vertex_x", "vertex_v", "vertex_C", "quadrature_x", "quadrature_v", "quadrature_C",
+            "quadrature_F", "quadrature_d", "operator_x", "operator_v", "operator_C", "cube_x", "cube_v",
+            "cube_C"]
+    for g in (0, 1):
+        rec["loss_w%d" % g] = window_loss(m, g)
+        for k in keys:
+            rec["w%d_%s" % (g, k)] = getattr(m, k).to_numpy()
+        rec["w%d_distances" % g] = m.distances.to_numpy()
+    rec["initial_quadrature_d_inv"] = m.initial_quadrature_d_inv.to_numpy()
+    rec["lagrangian_mesh_element"] = m.lagrangian_mesh_element.to_numpy()
+    rec["grasp_point_pos"] = np.asarray(m.grasp_point_pos)
+    rec["target_pcd_array"] = np.asarray(m.target_pcd_array)
+    rec["soft_body_model_vertices"] = np.asarray(m.soft_body_model_vertices)
+    rec["cube_model"] = np.asarray(m.cube_model)
+    rec["operator_model_without_position"] = np.asarray(m.operator_model_without_position)
+    for name in ("dt", "n_grid", "dx", "inv_dx", "vertex_p_mass", "quadrature_p_mass", "quadrature_p_vol",
+                 "operator_p_mass", "cube_p_mass", "garment_surface_area", "max_steps", "n_actions",
+                 "grasper_group_size", "operator_update_interval", "grad_update_interval", "scene_scaling"):
+        rec["const_" + name] = np.asarray(getattr(m, name))
+    rec["params"] = np.array([PARAMS["E"], PARAMS["nu"], PARAMS["contact_stiffness"],
+                              PARAMS["shearing_stiffness"]])
+    rec["seed_op"], rec["seed_cube"] = SEED_OP, SEED_CUBE
+    np.savez_compressed(out, **rec)
+
+
+def run_svd(tree, out):
+    m = import_reference(tree)
+    import ti_standin as ti
+    rng = np.random.default_rng(11)
+    mats = [np.eye(2), np.diag([1.3, 1.3]), np.array([[1.0, 1e-7], [0.0, 1.0 + 2e-7]]),
+            np.array([[0.9, 0.2], [-0.1, 1.1]]), np.array([[-0.8, 0.1], [0.3, 1.2]])]
+    mats += [np.eye(2) + 0.3 * rng.standard_normal((2, 2)) for _ in range(27)]
+    rows = {k: [] for k in ("A", "U", "S", "V", "gU", "gS", "gV", "out")}
+    for A in mats:
+        A = A.astype(np.float32)
+        U, S, V = ti.svd(A)
+        gU = rng.standard_normal((2, 2)).astype(np.float32)
+        gV = rng.standard_normal((2, 2)).astype(np.float32)
+        gS = np.diag(rng.standard_normal(2)).astype(np.float32)
+        res = m.backward_inplane_svd(gU.view(ti.TiArr), gS.view(ti.TiArr), gV.view(ti.TiArr), U, S, V)
+        for k, v in zip(rows, (A, U, S, V, gU, gS, gV, res)):
+            rows[k].append(np.asarray(v))
+    np.savez_compressed(out, **{k: np.stack(v) for k, v in rows.items()})
+
+
+def run_fd64(tree, out):
+    m = import_reference(tree, f64=True)
+    rec = {}
+    base = dict(PARAMS)
+    set_params(m, base)
+    rec["loss"] = window_loss(m, 0)
+    for name in ("E", "nu", "contact_stiffness", "shearing_stiffness"):
+        h = 1e-5 * base[name]
+        vals = []
+        for sgn in (1, -1):
+            p = dict(base)
+            p[name] = base[name] + sgn * h
+            set_params(m, p)
+            vals.append(window_loss(m, 0))
+        rec["fd_" + name] = (vals[0] - vals[1]) / (2 * h)
+        set_params(m, base)
+    coords = [(3, 0, 1), (5, 1, 0)]
+    for (a, b, c) in coords:
+        h = 1e-6
+        vals = []
+        for sgn in (1, -1):
+            m.grasp_point_pos[a, b, c] += sgn * h
+            vals.append(window_loss(m, 0))
+            m.grasp_point_pos[a, b, c] -= sgn * h
+        rec["fd_seq_%d_%d_%d" % (a, b, c)] = (vals[0] - vals[1]) / (2 * h)
+    rec["params"] = np.array([base["E"], base["nu"], base["contact_stiffness"], base["shearing_stiffness"]])
+    np.savez_compressed(out, **rec)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--mode", default="all", choices=["all", "forward32", "svd", "fd64"])
+    ap.add_argument("--tree")
+    a = ap.parse_args()
+    if a.mode == "all":
+        tree = build_tree(a.ref)
+        try:
+            for mode in ("forward32", "svd", "fd64"):
+                t0 = time.time()
+                subprocess.run([sys.executable, __file__, "--mode", mode, "--tree", tree], check=True)
+                print("%s done in %.1f s" % (mode, time.time() - t0))
+        finally:
+            shutil.rmtree(tree, ignore_errors=True)
+        return
+    out = {"forward32": "ref_forward_f32.npz", "svd": "ref_svd_backward.npz", "fd64": "ref_fd_f64.npz"}[a.mode]
+    {"forward32": run_forward32, "svd": run_svd, "fd64": run_fd64}[a.mode](a.tree, os.path.join(HERE, out))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,114 @@
+"""Pins the oracle against golden vectors produced by the reference's own
+source (tests/golden/make_golden.py).  CPU only."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import sim64
+from oracle.sim64 import OracleSim, compute_loss, svd2_taichi, svd_backward_clamped
+from tests.ref_scene import small_reference_scene
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _load(name):
+    path = os.path.join(GOLD, name)
+    if not os.path.exists(path):
+        pytest.skip("golden file %s missing" % name)
+    return np.load(path)
+
+
+@pytest.fixture(scope="module")
+def scene():
+    return small_reference_scene()
+
+
+def _params(p, dtype):
+    return {"E": torch.tensor(p["E"], dtype=dtype), "nu": torch.tensor(p["nu"], dtype=dtype),
+            "ks": torch.tensor(p["shearing_stiffness"], dtype=dtype),
+            "kc": torch.tensor(p["contact_stiffness"], dtype=dtype)}
+
+
+def _window(scene, window, dtype=torch.float64, svd_grad="exact", params=None, seq=None):
+    const = scene["const"]
+    sim, st = OracleSim.initialize(const, scene["vertices"], scene["triangles"], scene["operator_x"],
+                                   scene["cube_x"], dtype=dtype, svd_grad=svd_grad)
+    if seq is None:
+        seq = torch.tensor(scene["grasp_point_pos"], dtype=dtype)
+    params = params or _params(scene["params"], dtype)
+    states = sim64.rollout(sim, st, scene["max_steps"] - 1, params, seq=seq, window=window, keep_states=True)
+    targets = torch.tensor(scene["targets"][window], dtype=dtype)
+    loss, arg = compute_loss(states[scene["max_steps"] - 3]["vx"], targets)
+    return sim, states, loss, arg
+
+
+def test_scene_constants_match_reference(scene):
+    g = _load("ref_forward_f32.npz")
+    c = scene["const"]
+    assert c.n_grid == int(g["const_n_grid"])
+    for name in ("vertex_p_mass", "quadrature_p_mass", "quadrature_p_vol", "operator_p_mass", "cube_p_mass"):
+        assert getattr(c, name) == pytest.approx(float(g["const_" + name]), rel=1e-14), name
+    assert scene["area"] == pytest.approx(float(g["const_garment_surface_area"]), rel=1e-14)
+    assert scene["max_steps"] == int(g["const_max_steps"])
+    assert c.n_actions == int(g["const_n_actions"])
+    assert c.grasper_group_size == int(g["const_grasper_group_size"])
+    np.testing.assert_allclose(scene["vertices"], g["soft_body_model_vertices"], rtol=0, atol=1e-15)
+    np.testing.assert_allclose(scene["cube_x"], g["cube_model"], rtol=0, atol=1e-15)
+    np.testing.assert_allclose(scene["grasp_point_pos"], g["grasp_point_pos"], rtol=0, atol=1e-15)
+    np.testing.assert_allclose(scene["targets"], g["target_pcd_array"], rtol=0, atol=1e-15)
+
+
+@pytest.mark.parametrize("window", [0, 1])
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_forward_matches_reference_source(scene, window, dtype):
+    g = _load("ref_forward_f32.npz")
+    sim, states, loss, _ = _window(scene, window, dtype)
+    np.testing.assert_allclose(sim.D0inv.numpy(), g["initial_quadrature_d_inv"], rtol=1e-5, atol=1e-3)
+    steps = scene["max_steps"]
+    key = {"vx": "vertex_x", "vv": "vertex_v", "vC": "vertex_C", "qx": "quadrature_x", "qv": "quadrature_v",
+           "qC": "quadrature_C", "qF": "quadrature_F", "qd": "quadrature_d", "ox": "operator_x",
+           "ov": "operator_v", "oC": "operator_C", "cx": "cube_x", "cv": "cube_v", "cC": "cube_C"}
+    for f in range(steps):
+        for k, name in key.items():
+            ref = g["w%d_%s" % (window, name)][f]
+            got = states[f][k].detach().numpy()
+            scale = max(np.abs(ref).max(), 1e-6)
+            err = np.abs(got - ref).max() / scale
+            assert err < 2e-4, (f, k, err)
+    assert float(loss) == pytest.approx(float(g["loss_w%d" % window]), rel=1e-4)
+
+
+def test_svd_convention_and_clamped_backward():
+    g = _load("ref_svd_backward.npz")
+    A = torch.tensor(g["A"], dtype=torch.float64)
+    U, S, V = svd2_taichi(A)
+    np.testing.assert_allclose(U.numpy(), g["U"], atol=2e-6)
+    np.testing.assert_allclose(S.numpy(), g["S"], atol=2e-6)
+    np.testing.assert_allclose(V.numpy(), g["V"], atol=2e-6)
+    t = {k: torch.tensor(g[k], dtype=torch.float64) for k in ("U", "S", "V", "gU", "gS", "gV")}
+    out = svd_backward_clamped(t["gU"], t["gS"], t["gV"], t["U"], t["S"], t["V"]).numpy()
+    ref = g["out"]
+    scale = np.maximum(np.abs(ref).max(axis=(1, 2), keepdims=True), 1.0)
+    assert (np.abs(out - ref) / scale).max() < 1e-4
+
+
+def test_oracle_gradients_match_fd_of_reference_source(scene):
+    g = _load("ref_fd_f64.npz")
+    p = {"E": float(g["params"][0]), "nu": float(g["params"][1]), "contact_stiffness": float(g["params"][2]),
+         "shearing_stiffness": float(g["params"][3])}
+    params = {k: v.clone().requires_grad_(True) for k, v in _params(p, torch.float64).items()}
+    seq = torch.tensor(scene["grasp_point_pos"], dtype=torch.float64, requires_grad=True)
+    _, _, loss, _ = _window(scene, 0, params=params, seq=seq)
+    assert float(loss) == pytest.approx(float(g["loss"]), rel=1e-12)
+    loss.backward()
+    for k, ref in (("E", "fd_E"), ("nu", "fd_nu"), ("kc", "fd_contact_stiffness"), ("ks", "fd_shearing_stiffness")):
+        got = float(params[k].grad)
+        fd = float(g[ref])
+        assert got == pytest.approx(fd, rel=2e-4, abs=1e-12), (k, got, fd)
+    for name in g.files:
+        if name.startswith("fd_seq_"):
+            a, b, c = (int(t) for t in name[len("fd_seq_"):].split("_"))
+            got = float(seq.grad[a, b, c])
+            assert got == pytest.approx(float(g[name]), rel=2e-4, abs=1e-12), (name, got, float(g[name]))
