@@ -1,0 +1,1129 @@
+// sm_100a kernels of the batched codimensional-cloth MPM substep, its adjoint
+// and the Chamfer loss.  One CTA processes one chunk: a contiguous,
+// mesh-ordered range of one particle species of one cloth instance.
+//
+// Forward substep (simulation.py:480-488, forward):
+//   k_tri_forward    in-plane QR + rotation factor + stress of every triangle
+//                    (simulation.py:24-28, 39-42, 214-240), its own-node APIC
+//                    scatter and normal force (simulation.py:193-265), and the
+//                    per-corner in-plane forces (simulation.py:266-271) written
+//                    to a buffer instead of being scattered at the vertices'
+//                    stencils (see k_point_p2g)
+//   k_point_p2g      vertex / operator / cube APIC scatter (simulation.py:139-191);
+//                    a vertex adds the sum of its triangles' corner forces, which
+//                    equals the reference's per-triangle scatter with the
+//                    vertex's weights (the weights depend only on the vertex)
+//   k_grid           grid update and walls (simulation.py:274-302) on active
+//                    blocks only
+//   k_g2p            G2P for all species + triangle state update
+//                    (simulation.py:304-430)
+// Reverse substep: k_g2p_adj, k_grid_adj, k_point_adj, k_tri_adj, k_vertex_collect.
+#include <cuda_runtime.h>
+
+#include "dcp_internal.cuh"
+#include "dcp_launch.h"
+
+namespace dcp {
+
+__device__ __forceinline__ float3 ld3(const float* base, long long stride, long long i) {
+  return make_float3(__ldg(base + i), __ldg(base + stride + i), __ldg(base + 2 * stride + i));
+}
+
+// ============================================================== init
+// initialize_ti_field (simulation.py:447-477): zero velocities and affine
+// matrices, triangle d = [e1, e2, n] with n the normalised cross product of the
+// eps-normalised edges (norm(1e-6)), rest-shape inverse D0^-1.
+__global__ void k_init(BatchDev B, const float* __restrict__ x0v, const float* __restrict__ x0o,
+                       const float* __restrict__ x0c, float* __restrict__ state, float* __restrict__ rest) {
+  StateP S = state_ptrs(state, B.nv, B.nt, B.no);
+  const long long total = (long long)B.nv + B.no + B.nc + B.nt;
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
+    long long i = g;
+    if (i < B.nv + B.no + B.nc) {
+      float* dst;
+      const float* src;
+      long long n, p;
+      if (i < B.nv) { dst = S.v; src = x0v; n = B.nv; p = i; }
+      else if (i < B.nv + B.no) { dst = S.o; src = x0o; n = B.no; p = i - B.nv; }
+      else { dst = S.c; src = x0c; n = B.nc; p = i - B.nv - B.no; }
+      for (int c = 0; c < 3; ++c) dst[c * n + p] = src[c * n + p];
+      for (int c = 3; c < 15; ++c) dst[c * n + p] = 0.f;
+      continue;
+    }
+    const long long t = i - (B.nv + B.no + B.nc);
+    const int a = B.tri_v[t], b = B.tri_v[B.nt + t], c = B.tri_v[2 * (long long)B.nt + t];
+    const long long nv = B.nv;
+    const float ax = x0v[a], ay = x0v[nv + a], az = x0v[2 * nv + a];
+    const float d1x = x0v[b] - ax, d1y = x0v[nv + b] - ay, d1z = x0v[2 * nv + b] - az;
+    const float d2x = x0v[c] - ax, d2y = x0v[nv + c] - ay, d2z = x0v[2 * nv + c] - az;
+    const float l1 = sqrtf(d1x * d1x + d1y * d1y + d1z * d1z + 1e-6f);
+    const float l2 = sqrtf(d2x * d2x + d2y * d2y + d2z * d2z + 1e-6f);
+    const float n1x = d1x / l1, n1y = d1y / l1, n1z = d1z / l1;
+    const float n2x = d2x / l2, n2y = d2y / l2, n2z = d2z / l2;
+    float nx = n1y * n2z - n1z * n2y, ny = n1z * n2x - n1x * n2z, nz = n1x * n2y - n1y * n2x;
+    const float l3 = sqrtf(nx * nx + ny * ny + nz * nz + 1e-6f);
+    nx /= l3; ny /= l3; nz /= l3;
+    // D0 = [d1 d2 n] (columns); inverse by the adjugate
+    const float m00 = d1x, m01 = d2x, m02 = nx, m10 = d1y, m11 = d2y, m12 = ny, m20 = d1z, m21 = d2z, m22 = nz;
+    const float c00 = m11 * m22 - m12 * m21, c01 = m02 * m21 - m01 * m22, c02 = m01 * m12 - m02 * m11;
+    const float c10 = m12 * m20 - m10 * m22, c11 = m00 * m22 - m02 * m20, c12 = m02 * m10 - m00 * m12;
+    const float c20 = m10 * m21 - m11 * m20, c21 = m01 * m20 - m00 * m21, c22 = m00 * m11 - m01 * m10;
+    const float det = m00 * c00 + m01 * c10 + m02 * c20;
+    const float id = 1.f / det;
+    const float inv[9] = {c00 * id, c01 * id, c02 * id, c10 * id, c11 * id, c12 * id, c20 * id, c21 * id, c22 * id};
+    for (int q = 0; q < 9; ++q) {
+      rest[q * (long long)B.nt + t] = inv[q];
+      S.t[q * (long long)B.nt + t] = 0.f;
+    }
+    S.t[9 * (long long)B.nt + t] = nx;
+    S.t[10 * (long long)B.nt + t] = ny;
+    S.t[11 * (long long)B.nt + t] = nz;
+  }
+}
+
+// Triangle geometry at one state: vertex ids, positions, velocities, centroid.
+struct TriGeom {
+  int vid[3];
+  float X[3][3];  // [corner][axis]
+  float V[3][3];
+  float xc[3], vc[3];
+};
+__device__ __forceinline__ void load_tri(const BatchDev& B, const StateP& S, long long t, bool need_v, TriGeom& g) {
+  const long long nv = B.nv, nt = B.nt;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) g.vid[c] = __ldg(B.tri_v + c * nt + t);
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) g.X[c][a] = __ldg(S.v + a * nv + g.vid[c]);
+  const float third = 1.f / 3.f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) g.xc[a] = third * ((g.X[0][a] + g.X[1][a]) + g.X[2][a]);
+  if (need_v) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int a = 0; a < 3; ++a) g.V[c][a] = __ldg(S.v + (3 + a) * nv + g.vid[c]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) g.vc[a] = third * ((g.V[0][a] + g.V[1][a]) + g.V[2][a]);
+  }
+}
+
+// F = d D0^-1 with d = [x2 - x1, x3 - x1, d3] (simulation.py:395-407).
+__device__ __forceinline__ void tri_F(const TriGeom& g, const float d3[3], const float Di[9], M3<float>& d, M3<float>& F) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    d.m[3 * a + 0] = g.X[1][a] - g.X[0][a];
+    d.m[3 * a + 1] = g.X[2][a] - g.X[0][a];
+    d.m[3 * a + 2] = d3[a];
+  }
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      F.m[3 * r + c] = d.m[3 * r] * Di[c] + d.m[3 * r + 1] * Di[3 + c] + d.m[3 * r + 2] * Di[6 + c];
+}
+
+__device__ __forceinline__ void lame(float E, float nu, float& mu, float& la) {
+  mu = E / (2.f * (1.f + nu));
+  la = E * nu / ((1.f + nu) * (1.f - 2.f * nu));
+}
+
+// ============================================================== forward
+__global__ void __launch_bounds__(256) k_tri_forward(BatchDev B, const float* __restrict__ params,
+                                                     const float* __restrict__ rest, const float* __restrict__ sin) {
+  extern __shared__ float4 tile[];
+  __shared__ TileHdr T;
+  const Chunk ch = B.chunks[blockIdx.x];
+  const InstDev& I = B.inst[ch.inst];
+  const bool valid = threadIdx.x < ch.count;
+  const long long t = ch.start + threadIdx.x;
+  const long long nt = B.nt;
+  StateP S = state_ptrs(const_cast<float*>(sin), B.nv, B.nt, B.no);
+  TriGeom g;
+  Sten st;
+  if (valid) {
+    load_tri(B, S, t, true, g);
+    make_stencil(g.xc, I, st, B.status, ch.inst);
+  }
+  tile_setup(T, st.base, valid, B.tile_nodes);
+  if (!T.use && T.any && threadIdx.x == 0) atomicOr(B.status + ch.inst, STATUS_TILE_FALLBACK);
+  tile_zero(tile, T);
+  __syncthreads();
+  if (valid) {
+    const float* prm = params + ch.inst * PRM_STRIDE;
+    float mu, la;
+    lame(prm[PRM_E], prm[PRM_NU], mu, la);
+    const float ks = prm[PRM_KS], kc = prm[PRM_KC];
+    float C[9], d3[3], Di[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) C[q] = __ldg(S.t + q * nt + t);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) d3[q] = __ldg(S.t + (9 + q) * nt + t);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) Di[q] = __ldg(rest + q * nt + t);
+    M3<float> d, F;
+    tri_F(g, d3, Di, d, F);
+    Stress<float> sts;
+    stress_forward<float>(F, mu, la, ks, kc, sts);
+    const M3<float>& P = sts.P;
+    const float vol = I.vol_q, dt = B.dt, m = I.m_q, dx = I.dx, inv_dx = I.inv_dx;
+    // per-corner in-plane forces with r1 = (D0^-1[0,0], d[0,1], d[0,2]),
+    // r2 = (D0^-1[1,0], d[1,1], d[1,2]) as in simulation.py:247-248
+    const V3<float> r1 = v3(Di[0], d.m[1], d.m[2]);
+    const V3<float> r2 = v3(Di[3], d.m[4], d.m[5]);
+    const float k = vol * dt;
+    const V3<float> f1 = k * matvec(P, r1 + r2);
+    const V3<float> f2 = (-k) * matvec(P, r1);
+    const V3<float> f3 = (-k) * matvec(P, r2);
+    const long long e3 = 3 * nt;
+    B.force[0 * e3 + 0 * nt + t] = f1.x; B.force[1 * e3 + 0 * nt + t] = f1.y; B.force[2 * e3 + 0 * nt + t] = f1.z;
+    B.force[0 * e3 + 1 * nt + t] = f2.x; B.force[1 * e3 + 1 * nt + t] = f2.y; B.force[2 * e3 + 1 * nt + t] = f2.z;
+    B.force[0 * e3 + 2 * nt + t] = f3.x; B.force[1 * e3 + 2 * nt + t] = f3.y; B.force[2 * e3 + 2 * nt + t] = f3.z;
+    // own-node APIC momentum + normal force (simulation.py:250-265)
+    const float mvx = m * g.vc[0], mvy = m * g.vc[1], mvz = m * g.vc[2];
+    float A[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) A[q] = C[q] * m;
+    const float cn = -vol * dt;
+    const float P3x = P.m[2], P3y = P.m[5], P3z = P.m[8];
+#pragma unroll
+    for (int oi = 0; oi < 3; ++oi)
+#pragma unroll
+      for (int oj = 0; oj < 3; ++oj)
+#pragma unroll
+        for (int ok = 0; ok < 3; ++ok) {
+          const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
+          const float gx = st.dw[0][oi] * inv_dx * st.w[1][oj] * st.w[2][ok];
+          const float gy = st.w[0][oi] * (st.dw[1][oj] * inv_dx) * st.w[2][ok];
+          const float gz = st.w[0][oi] * st.w[1][oj] * (st.dw[2][ok] * inv_dx);
+          const float px = ((float)oi - st.fx[0]) * dx, py = ((float)oj - st.fx[1]) * dx, pz = ((float)ok - st.fx[2]) * dx;
+          const float nrm = cn * (gx * d3[0] + gy * d3[1] + gz * d3[2]);
+          float4 val;
+          val.x = W * (mvx + (A[0] * px + A[1] * py + A[2] * pz)) + nrm * P3x;
+          val.y = W * (mvy + (A[3] * px + A[4] * py + A[5] * pz)) + nrm * P3y;
+          val.z = W * (mvz + (A[6] * px + A[7] * py + A[8] * pz)) + nrm * P3z;
+          val.w = W * m;
+          emit<true>(tile, T, B, I, ch.inst, st.base[0] + oi, st.base[1] + oj, st.base[2] + ok, val);
+        }
+  }
+  __syncthreads();
+  if (T.use) tile_flush<true>(tile, T, B, I, ch.inst);
+}
+
+__device__ __forceinline__ void point_arrays(const BatchDev& B, const StateP& S, int kind, float*& base, long long& n) {
+  if (kind == CHUNK_VERTEX) { base = S.v; n = B.nv; }
+  else if (kind == CHUNK_OPERATOR) { base = S.o; n = B.no; }
+  else { base = S.c; n = B.nc; }
+}
+
+// Operator target velocity of simulation.py:160-165 (keyframe index in float32).
+__device__ __forceinline__ bool operator_velocity(const BatchDev& B, const InstDev& I, const float* traj, int step,
+                                                  int window, long long p, float v[3], long long& i0, long long& i1) {
+  const float tt = (float)step * B.dt;
+  const int frame = (int)(tt / I.interval) + I.frames_per_window * window;
+  const int gid = (int)((p - I.o_off) / I.group_size);
+  v[0] = v[1] = v[2] = 0.f;
+  if (frame + 1 < I.n_actions && frame >= 0) {
+    i0 = I.traj_off + ((long long)frame * I.n_grip + gid) * 3;
+    i1 = I.traj_off + ((long long)(frame + 1) * I.n_grip + gid) * 3;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) v[a] = (__ldg(traj + i1 + a) - __ldg(traj + i0 + a)) / I.interval;
+    return true;
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(256) k_point_p2g(BatchDev B, const float* __restrict__ traj, int step, int window,
+                                                   const float* __restrict__ sin) {
+  extern __shared__ float4 tile[];
+  __shared__ TileHdr T;
+  const Chunk ch = B.chunks[B.n_tri_chunks + blockIdx.x];
+  const InstDev& I = B.inst[ch.inst];
+  const bool valid = threadIdx.x < ch.count;
+  const long long p = ch.start + threadIdx.x;
+  StateP S = state_ptrs(const_cast<float*>(sin), B.nv, B.nt, B.no);
+  float* arr;
+  long long n;
+  point_arrays(B, S, ch.kind, arr, n);
+  float X[3];
+  Sten st;
+  if (valid) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) X[a] = __ldg(arr + a * n + p);
+    make_stencil(X, I, st, B.status, ch.inst);
+  }
+  tile_setup(T, st.base, valid, B.tile_nodes);
+  if (!T.use && T.any && threadIdx.x == 0) atomicOr(B.status + ch.inst, STATUS_TILE_FALLBACK);
+  tile_zero(tile, T);
+  __syncthreads();
+  if (valid) {
+    float m, base_v[3] = {0.f, 0.f, 0.f};
+    if (ch.kind == CHUNK_VERTEX) {
+      m = I.m_v;
+      float f[3] = {0.f, 0.f, 0.f};
+      const long long e3 = 3LL * B.nt;
+      const int e0 = __ldg(B.inc_ptr + p), e1 = __ldg(B.inc_ptr + p + 1);
+      for (int e = e0; e < e1; ++e) {
+        const int id = __ldg(B.inc_e + e);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) f[a] += B.force[a * e3 + id];
+      }
+      // temp_v = v + (0, dt*scene_scaling*g, 0) (simulation.py:182)
+      base_v[0] = m * __ldg(arr + 3 * n + p) + f[0];
+      base_v[1] = m * (__ldg(arr + 4 * n + p) + I.gravity_dv) + f[1];
+      base_v[2] = m * __ldg(arr + 5 * n + p) + f[2];
+    } else if (ch.kind == CHUNK_OPERATOR) {
+      m = I.m_o;
+      float v[3];
+      long long i0, i1;
+      operator_velocity(B, I, traj, step, window, p, v, i0, i1);
+      base_v[0] = m * v[0]; base_v[1] = m * v[1]; base_v[2] = m * v[2];
+    } else {
+      m = I.m_c;  // cube: affine momentum only (simulation.py:150-152)
+    }
+    float A[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) A[q] = m * __ldg(arr + (6 + q) * n + p);
+    const float dx = I.dx;
+#pragma unroll
+    for (int oi = 0; oi < 3; ++oi)
+#pragma unroll
+      for (int oj = 0; oj < 3; ++oj)
+#pragma unroll
+        for (int ok = 0; ok < 3; ++ok) {
+          const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
+          const float px = ((float)oi - st.fx[0]) * dx, py = ((float)oj - st.fx[1]) * dx, pz = ((float)ok - st.fx[2]) * dx;
+          float4 val;
+          val.x = W * (base_v[0] + (A[0] * px + A[1] * py + A[2] * pz));
+          val.y = W * (base_v[1] + (A[3] * px + A[4] * py + A[5] * pz));
+          val.z = W * (base_v[2] + (A[6] * px + A[7] * py + A[8] * pz));
+          val.w = W * m;
+          emit<true>(tile, T, B, I, ch.inst, st.base[0] + oi, st.base[1] + oj, st.base[2] + ok, val);
+        }
+  }
+  __syncthreads();
+  if (T.use) tile_flush<true>(tile, T, B, I, ch.inst);
+}
+
+// Node coordinates of lane l (0..63) of an active block.
+__device__ __forceinline__ void block_node(const InstDev& I, int blk, int l, int& i, int& j, int& k) {
+  const int lb = blk - (int)(I.node_off >> 6);
+  const int nb = I.nb;
+  const int bi = lb / (nb * nb), bj = (lb / nb) % nb, bk = lb % nb;
+  i = bi * 4 + (l >> 4);
+  j = bj * 4 + ((l >> 2) & 3);
+  k = bk * 4 + (l & 3);
+}
+
+// Kinematic sphere gripper (build extension): returns the index of the last
+// gripper whose sphere contains node (i, j, k), or -1.
+__device__ __forceinline__ int kinematic_hit(const InstDev& I, const float* traj, int step, int i, int j, int k) {
+  if (I.grip_mode != GRIP_KINEMATIC || step >= I.n_traj_steps) return -1;
+  const float px = i * I.dx, py = j * I.dx, pz = k * I.dx;
+  const float r2 = I.grip_radius * I.grip_radius;
+  const long long cbase = I.traj_off + (long long)I.n_traj_steps * I.n_grip * 3;
+  int hit = -1;
+  for (int q = 0; q < I.n_grip; ++q) {
+    const long long o = cbase + ((long long)step * I.n_grip + q) * 3;
+    const float dx = px - __ldg(traj + o), dy = py - __ldg(traj + o + 1), dz = pz - __ldg(traj + o + 2);
+    if (dx * dx + dy * dy + dz * dz <= r2) hit = q;
+  }
+  return hit;
+}
+
+__global__ void __launch_bounds__(256) k_grid(BatchDev B, const float* __restrict__ params,
+                                              const float* __restrict__ traj, int step, int mode) {
+  const int count = B.counters[0];
+  const int per = blockDim.x >> 6, l = threadIdx.x & 63;
+  for (int item = blockIdx.x * per + (threadIdx.x >> 6); item < count; item += gridDim.x * per) {
+    const int blk = B.list_blk[item], inst = B.list_inst[item];
+    const InstDev& I = B.inst[inst];
+    int i, j, k;
+    block_node(I, blk, l, i, j, k);
+    const long long n = (long long)blk * 64 + l;
+    const float4 pm = B.grid_pm[n];
+    const float inv_m = 1.f / (pm.w + 1e-9f);
+    const float v[3] = {inv_m * pm.x, inv_m * pm.y, inv_m * pm.z};
+    float out[3];
+    grid_bc<float>(v, i, j, k, I.G, I.bound, __ldg(params + inst * PRM_STRIDE + PRM_FRICTION), out);
+    const int hit = kinematic_hit(I, traj, step, i, j, k);
+    if (hit >= 0) {
+      const long long o = I.traj_off + ((long long)step * I.n_grip + hit) * 3;
+      out[0] = __ldg(traj + o); out[1] = __ldg(traj + o + 1); out[2] = __ldg(traj + o + 2);
+    }
+    B.grid_v[n] = make_float4(out[0], out[1], out[2], 0.f);
+    if (mode == GRID_FORWARD) {
+      B.grid_pm[n] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (l == 0) B.flags[blk] = 0u;
+    } else {
+      B.grid_adj[n] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
+}
+
+__device__ __forceinline__ float3 gv(const BatchDev& B, const InstDev& I, int i, int j, int k) {
+  const float4 v = __ldg(B.grid_v + node_index(I, i, j, k));
+  return make_float3(v.x, v.y, v.z);
+}
+
+__global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict__ params,
+                                             const float* __restrict__ sin, float* __restrict__ sout) {
+  const Chunk ch = B.chunks[blockIdx.x];
+  if (threadIdx.x >= ch.count) return;
+  const InstDev& I = B.inst[ch.inst];
+  StateP Si = state_ptrs(const_cast<float*>(sin), B.nv, B.nt, B.no);
+  StateP So = state_ptrs(sout, B.nv, B.nt, B.no);
+  const float dt = B.dt, inv_dx = I.inv_dx;
+  if (ch.kind == CHUNK_TRI) {
+    const long long t = ch.start + threadIdx.x, nt = B.nt;
+    TriGeom g;
+    load_tri(B, Si, t, false, g);
+    Sten st;
+    make_stencil(g.xc, I, st, B.status, ch.inst);
+    float Ct[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int oi = 0; oi < 3; ++oi)
+#pragma unroll
+      for (int oj = 0; oj < 3; ++oj)
+#pragma unroll
+        for (int ok = 0; ok < 3; ++ok) {
+          const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
+          const float3 gn = gv(B, I, st.base[0] + oi, st.base[1] + oj, st.base[2] + ok);
+          const float dp[3] = {(float)oi - st.fx[0], (float)oj - st.fx[1], (float)ok - st.fx[2]};
+          const float s = 4.f * W * inv_dx;
+          const float ga[3] = {gn.x, gn.y, gn.z};
+#pragma unroll
+          for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) Ct[3 * a + b] += s * ga[a] * dp[b];
+        }
+    // C = skew + (1 - damping) sym (simulation.py:381-383)
+    const float keep = 1.f - __ldg(params + ch.inst * PRM_STRIDE + PRM_DAMPING);
+    float Cn[9];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const float sk = 0.5f * (Ct[3 * a + b] - Ct[3 * b + a]);
+        const float sy = 0.5f * (Ct[3 * a + b] + Ct[3 * b + a]);
+        Cn[3 * a + b] = sk + keep * sy;
+      }
+    float d3[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) d3[q] = __ldg(Si.t + (9 + q) * nt + t);
+    // d3 += (dt C + dt^2/2 C C) d3 (simulation.py:397-400)
+    float Md[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float acc = 0.f;
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        float cc = 0.f;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) cc += Cn[3 * a + q] * Cn[3 * q + b];
+        acc += (dt * Cn[3 * a + b] + 0.5f * dt * dt * cc) * d3[b];
+      }
+      Md[a] = acc;
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) So.t[q * nt + t] = Cn[q];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) So.t[(9 + q) * nt + t] = d3[q] + Md[q];
+    return;
+  }
+  float *ai, *ao;
+  long long n;
+  point_arrays(B, Si, ch.kind, ai, n);
+  point_arrays(B, So, ch.kind, ao, n);
+  const long long p = ch.start + threadIdx.x;
+  float X[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) X[a] = __ldg(ai + a * n + p);
+  Sten st;
+  make_stencil(X, I, st, B.status, ch.inst);
+  float v[3] = {0.f, 0.f, 0.f}, C[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int oi = 0; oi < 3; ++oi)
+#pragma unroll
+    for (int oj = 0; oj < 3; ++oj)
+#pragma unroll
+      for (int ok = 0; ok < 3; ++ok) {
+        const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
+        const float3 gn = gv(B, I, st.base[0] + oi, st.base[1] + oj, st.base[2] + ok);
+        const float dp[3] = {(float)oi - st.fx[0], (float)oj - st.fx[1], (float)ok - st.fx[2]};
+        const float ga[3] = {gn.x, gn.y, gn.z};
+        const float s = 4.f * W * inv_dx;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          v[a] += W * ga[a];
+#pragma unroll
+          for (int b = 0; b < 3; ++b) C[3 * a + b] += s * ga[a] * dp[b];
+        }
+      }
+  bool finite = true;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    ao[a * n + p] = X[a] + dt * v[a];
+    ao[(3 + a) * n + p] = v[a];
+    finite = finite && isfinite(v[a]);
+  }
+#pragma unroll
+  for (int q = 0; q < 9; ++q) ao[(6 + q) * n + p] = C[q];
+  if (!finite) atomicOr(B.status + ch.inst, STATUS_NONFINITE);
+}
+
+// ============================================================== adjoint
+// Reverse of k_g2p: scatter dL/dv_out into the adjoint grid and accumulate
+// the position adjoint of the gather; triangle: reverse of the d3 update and of
+// the skew/sym damping.
+__global__ void __launch_bounds__(256) k_g2p_adj(BatchDev B, const float* __restrict__ params,
+                                                 const float* __restrict__ sin, const float* __restrict__ aout,
+                                                 float* __restrict__ ain, double* __restrict__ gparams) {
+  extern __shared__ float4 tile[];
+  __shared__ TileHdr T;
+  const Chunk ch = B.chunks[blockIdx.x];
+  const InstDev& I = B.inst[ch.inst];
+  const bool valid = threadIdx.x < ch.count;
+  StateP Si = state_ptrs(const_cast<float*>(sin), B.nv, B.nt, B.no);
+  StateP Ao = state_ptrs(const_cast<float*>(aout), B.nv, B.nt, B.no);
+  StateP Ai = state_ptrs(ain, B.nv, B.nt, B.no);
+  const float dt = B.dt, inv_dx = I.inv_dx;
+  const bool tri = ch.kind == CHUNK_TRI;
+  const long long idx = ch.start + threadIdx.x;
+  float X[3];
+  TriGeom g;
+  Sten st;
+  float *ai = nullptr, *ao = nullptr, *aa = nullptr;
+  long long n = 0;
+  if (!tri) {
+    point_arrays(B, Si, ch.kind, ai, n);
+    point_arrays(B, Ao, ch.kind, ao, n);
+    point_arrays(B, Ai, ch.kind, aa, n);
+  }
+  if (valid) {
+    if (tri) {
+      load_tri(B, Si, idx, false, g);
+      X[0] = g.xc[0]; X[1] = g.xc[1]; X[2] = g.xc[2];
+    } else {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) X[a] = __ldg(ai + a * n + idx);
+    }
+    make_stencil(X, I, st, B.status, ch.inst);
+  }
+  tile_setup(T, st.base, valid, B.tile_nodes);
+  tile_zero(tile, T);
+  __syncthreads();
+  float gdamp[1] = {0.f};
+  if (valid) {
+    // gather the grid velocities of the stencil once
+    float3 gn[27];
+#pragma unroll
+    for (int q = 0; q < 27; ++q) gn[q] = gv(B, I, st.base[0] + q / 9, st.base[1] + (q / 3) % 3, st.base[2] + q % 3);
+    float bC[9];  // adjoint of the gathered C (4 inv_dx sum W g (x) dpos)
+    float bV[3] = {0.f, 0.f, 0.f};
+    float bx[3] = {0.f, 0.f, 0.f};
+    if (tri) {
+      const long long nt = B.nt;
+      float Ct[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int q = 0; q < 27; ++q) {
+        const int oi = q / 9, oj = (q / 3) % 3, ok = q % 3;
+        const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
+        const float dp[3] = {(float)oi - st.fx[0], (float)oj - st.fx[1], (float)ok - st.fx[2]};
+        const float ga[3] = {gn[q].x, gn[q].y, gn[q].z};
+        const float s = 4.f * W * inv_dx;
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int b = 0; b < 3; ++b) Ct[3 * a + b] += s * ga[a] * dp[b];
+      }
+      const float damping = __ldg(params + ch.inst * PRM_STRIDE + PRM_DAMPING);
+      const float keep = 1.f - damping;
+      float Cn[9], sym[9];
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          sym[3 * a + b] = 0.5f * (Ct[3 * a + b] + Ct[3 * b + a]);
+          Cn[3 * a + b] = 0.5f * (Ct[3 * a + b] - Ct[3 * b + a]) + keep * sym[3 * a + b];
+        }
+      float d3[3], bd3o[3], bCo[9];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        d3[q] = __ldg(Si.t + (9 + q) * nt + idx);
+        bd3o[q] = __ldg(Ao.t + (9 + q) * nt + idx);
+      }
+#pragma unroll
+      for (int q = 0; q < 9; ++q) bCo[q] = __ldg(Ao.t + q * nt + idx);
+      // M = dt C + dt^2/2 C C ; d3' = d3 + M d3
+      float Mm[9];
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          float cc = 0.f;
+#pragma unroll
+          for (int q = 0; q < 3; ++q) cc += Cn[3 * a + q] * Cn[3 * q + b];
+          Mm[3 * a + b] = dt * Cn[3 * a + b] + 0.5f * dt * dt * cc;
+        }
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        float acc = bd3o[b];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) acc += Mm[3 * a + b] * bd3o[a];
+        Ai.t[(9 + b) * nt + idx] = acc;  // partial; k_tri_adj adds the P2G part
+      }
+      // dL/dC' = bCo + dt G + dt^2/2 (G C'^T + C'^T G), G = bd3' d3^T
+      float G[9];
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) G[3 * a + b] = bd3o[a] * d3[b];
+      float bCn[9];
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          float gc = 0.f, cg = 0.f;
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            gc += G[3 * a + q] * Cn[3 * b + q];
+            cg += Cn[3 * q + a] * G[3 * q + b];
+          }
+          bCn[3 * a + b] = bCo[3 * a + b] + dt * G[3 * a + b] + 0.5f * dt * dt * (gc + cg);
+        }
+      float gd = 0.f;
+#pragma unroll
+      for (int q = 0; q < 9; ++q) gd -= bCn[q] * sym[q];
+      gdamp[0] = gd;
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+          bC[3 * a + b] = 0.5f * (bCn[3 * a + b] - bCn[3 * b + a]) + keep * 0.5f * (bCn[3 * a + b] + bCn[3 * b + a]);
+    } else {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        bx[a] = __ldg(ao + a * n + idx);
+        bV[a] = __ldg(ao + (3 + a) * n + idx) + dt * bx[a];
+      }
+#pragma unroll
+      for (int q = 0; q < 9; ++q) bC[q] = __ldg(ao + (6 + q) * n + idx);
+    }
+    float px[3] = {0.f, 0.f, 0.f};
+    const float c4 = 4.f * inv_dx;
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+      const int oi = q / 9, oj = (q / 3) % 3, ok = q % 3;
+      const float w0 = st.w[0][oi], w1 = st.w[1][oj], w2 = st.w[2][ok];
+      const float W = w0 * w1 * w2;
+      const float gW[3] = {st.dw[0][oi] * w1 * w2 * inv_dx, w0 * st.dw[1][oj] * w2 * inv_dx, w0 * w1 * st.dw[2][ok] * inv_dx};
+      const float dp[3] = {(float)oi - st.fx[0], (float)oj - st.fx[1], (float)ok - st.fx[2]};
+      const float ga[3] = {gn[q].x, gn[q].y, gn[q].z};
+      float bg[3];
+      float s1 = bV[0] * ga[0] + bV[1] * ga[1] + bV[2] * ga[2];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const float cd = bC[3 * a] * dp[0] + bC[3 * a + 1] * dp[1] + bC[3 * a + 2] * dp[2];
+        bg[a] = W * (bV[a] + c4 * cd);
+        s1 += c4 * ga[a] * cd;
+      }
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const float cg = bC[b] * ga[0] + bC[3 + b] * ga[1] + bC[6 + b] * ga[2];
+        px[b] += s1 * gW[b] - c4 * inv_dx * W * cg;
+      }
+      emit<false>(tile, T, B, I, ch.inst, st.base[0] + oi, st.base[1] + oj, st.base[2] + ok,
+                  make_float4(bg[0], bg[1], bg[2], 0.f));
+    }
+    if (tri) {
+      const long long nt = B.nt;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) B.tri_tmp[a * nt + idx] = px[a];
+    } else {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) aa[a * n + idx] = bx[a] + px[a];
+    }
+  }
+  __syncthreads();
+  if (T.use) tile_flush<false>(tile, T, B, I, ch.inst);
+  if (tri) block_sum_atomic<1>(gdamp, gparams + ch.inst * PRM_STRIDE + PRM_DAMPING);
+}
+
+// Reverse of k_grid: dL/dp, dL/dm of every active node from dL/dv_out.
+__global__ void __launch_bounds__(256) k_grid_adj(BatchDev B, const float* __restrict__ params,
+                                                  const float* __restrict__ traj, int step, double* __restrict__ gparams,
+                                                  double* __restrict__ gtraj) {
+  const int count = B.counters[0];
+  const int per = blockDim.x >> 6, l = threadIdx.x & 63;
+  for (int item = blockIdx.x * per + (threadIdx.x >> 6); item < count; item += gridDim.x * per) {
+    const int blk = B.list_blk[item], inst = B.list_inst[item];
+    const InstDev& I = B.inst[inst];
+    int i, j, k;
+    block_node(I, blk, l, i, j, k);
+    const long long n = (long long)blk * 64 + l;
+    const float4 pm = B.grid_pm[n];
+    const float4 ga = B.grid_adj[n];
+    const float inv_m = 1.f / (pm.w + 1e-9f);
+    const float v[3] = {inv_m * pm.x, inv_m * pm.y, inv_m * pm.z};
+    const float mu_g = __ldg(params + inst * PRM_STRIDE + PRM_FRICTION);
+    float out[3];
+    const NodeBC<float> r = grid_bc<float>(v, i, j, k, I.G, I.bound, mu_g, out);
+    float bv[3] = {0.f, 0.f, 0.f};
+    float gmu = 0.f;
+    const float gout[3] = {ga.x, ga.y, ga.z};
+    const int hit = kinematic_hit(I, traj, step, i, j, k);
+    if (hit >= 0) {
+      const long long o = I.traj_off + ((long long)step * I.n_grip + hit) * 3;
+      if (ga.x != 0.f) atomicAdd(gtraj + o, (double)ga.x);
+      if (ga.y != 0.f) atomicAdd(gtraj + o + 1, (double)ga.y);
+      if (ga.z != 0.f) atomicAdd(gtraj + o + 2, (double)ga.z);
+    } else {
+      grid_bc_backward<float>(v, r, mu_g, gout, bv, gmu);
+    }
+    const float bp[3] = {inv_m * bv[0], inv_m * bv[1], inv_m * bv[2]};
+    const float bm = -inv_m * (bv[0] * v[0] + bv[1] * v[1] + bv[2] * v[2]);
+    B.grid_adj[n] = make_float4(bp[0], bp[1], bp[2], bm);
+    B.grid_pm[n] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (l == 0) B.flags[blk] = 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) gmu += __shfl_xor_sync(0xffffffffu, gmu, o);
+    if ((threadIdx.x & 31) == 0 && gmu != 0.f) atomicAdd(gparams + inst * PRM_STRIDE + PRM_FRICTION, (double)gmu);
+  }
+}
+
+__device__ __forceinline__ float4 gadj(const BatchDev& B, const InstDev& I, int i, int j, int k) {
+  return __ldg(B.grid_adj + node_index(I, i, j, k));
+}
+
+// Reverse of k_point_p2g: gather dL/dp, dL/dm over the stencil.
+__global__ void __launch_bounds__(256) k_point_adj(BatchDev B, const float* __restrict__ traj, int step, int window,
+                                                   const float* __restrict__ sin, float* __restrict__ ain,
+                                                   double* __restrict__ gtraj) {
+  const Chunk ch = B.chunks[B.n_tri_chunks + blockIdx.x];
+  if (threadIdx.x >= ch.count) return;
+  const InstDev& I = B.inst[ch.inst];
+  StateP Si = state_ptrs(const_cast<float*>(sin), B.nv, B.nt, B.no);
+  StateP Ai = state_ptrs(ain, B.nv, B.nt, B.no);
+  float *ai, *aa;
+  long long n;
+  point_arrays(B, Si, ch.kind, ai, n);
+  point_arrays(B, Ai, ch.kind, aa, n);
+  const long long p = ch.start + threadIdx.x;
+  float X[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) X[a] = __ldg(ai + a * n + p);
+  Sten st;
+  make_stencil(X, I, st, B.status, ch.inst);
+  float m, base_v[3] = {0.f, 0.f, 0.f};
+  long long i0 = -1, i1 = -1;
+  bool op_active = false;
+  if (ch.kind == CHUNK_VERTEX) {
+    m = I.m_v;
+    float f[3] = {0.f, 0.f, 0.f};
+    const long long e3 = 3LL * B.nt;
+    const int e0 = __ldg(B.inc_ptr + p), e1 = __ldg(B.inc_ptr + p + 1);
+    for (int e = e0; e < e1; ++e) {
+      const int id = __ldg(B.inc_e + e);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) f[a] += B.force[a * e3 + id];
+    }
+    base_v[0] = m * __ldg(ai + 3 * n + p) + f[0];
+    base_v[1] = m * (__ldg(ai + 4 * n + p) + I.gravity_dv) + f[1];
+    base_v[2] = m * __ldg(ai + 5 * n + p) + f[2];
+  } else if (ch.kind == CHUNK_OPERATOR) {
+    m = I.m_o;
+    float v[3];
+    op_active = operator_velocity(B, I, traj, step, window, p, v, i0, i1);
+    base_v[0] = m * v[0]; base_v[1] = m * v[1]; base_v[2] = m * v[2];
+  } else {
+    m = I.m_c;
+  }
+  float Cm[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) Cm[q] = __ldg(ai + (6 + q) * n + p);
+  const float dx = I.dx, inv_dx = I.inv_dx;
+  float sp[3] = {0.f, 0.f, 0.f};     // sum W bp
+  float spd[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // sum W bp (x) dpos
+  float px[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+  for (int q = 0; q < 27; ++q) {
+    const int oi = q / 9, oj = (q / 3) % 3, ok = q % 3;
+    const float w0 = st.w[0][oi], w1 = st.w[1][oj], w2 = st.w[2][ok];
+    const float W = w0 * w1 * w2;
+    const float gW[3] = {st.dw[0][oi] * w1 * w2 * inv_dx, w0 * st.dw[1][oj] * w2 * inv_dx, w0 * w1 * st.dw[2][ok] * inv_dx};
+    const float dp[3] = {((float)oi - st.fx[0]) * dx, ((float)oj - st.fx[1]) * dx, ((float)ok - st.fx[2]) * dx};
+    const float4 g = gadj(B, I, st.base[0] + oi, st.base[1] + oj, st.base[2] + ok);
+    const float bp[3] = {g.x, g.y, g.z};
+    float s = g.w * m;
+    float ctb[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float pay = base_v[a] + m * (Cm[3 * a] * dp[0] + Cm[3 * a + 1] * dp[1] + Cm[3 * a + 2] * dp[2]);
+      s += bp[a] * pay;
+      sp[a] += W * bp[a];
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        spd[3 * a + b] += W * bp[a] * dp[b];
+        ctb[b] += Cm[3 * a + b] * bp[a];
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < 3; ++b) px[b] += s * gW[b] - W * m * ctb[b];
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) aa[a * n + p] += px[a];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) aa[(6 + q) * n + p] = m * spd[q];
+  if (ch.kind == CHUNK_VERTEX) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      aa[(3 + a) * n + p] = m * sp[a];
+      B.barf[a * (long long)B.nv + p] = sp[a];
+    }
+  } else {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) aa[(3 + a) * n + p] = 0.f;
+    if (ch.kind == CHUNK_OPERATOR && op_active) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const double gvt = (double)(m * sp[a]) / (double)I.interval;
+        if (gvt != 0.0) {
+          atomicAdd(gtraj + i1 + a, gvt);
+          atomicAdd(gtraj + i0 + a, -gvt);
+        }
+      }
+    }
+  }
+}
+
+// Reverse of k_tri_forward for one triangle: own-stencil gather, per-corner
+// force adjoints from dL/df of the three vertices, stress adjoint, and the
+// contributions to the three vertices (written per corner, summed by
+// k_vertex_collect).
+__global__ void __launch_bounds__(128) k_tri_adj(BatchDev B, const float* __restrict__ params,
+                                                 const float* __restrict__ rest, const float* __restrict__ sin,
+                                                 float* __restrict__ ain, double* __restrict__ gparams) {
+  const Chunk ch = B.chunks[blockIdx.x];
+  const InstDev& I = B.inst[ch.inst];
+  const bool valid = threadIdx.x < ch.count;
+  const long long t = ch.start + threadIdx.x, nt = B.nt;
+  StateP Si = state_ptrs(const_cast<float*>(sin), B.nv, B.nt, B.no);
+  StateP Ai = state_ptrs(ain, B.nv, B.nt, B.no);
+  const float* prm = params + ch.inst * PRM_STRIDE;
+  float E = prm[PRM_E], nu = prm[PRM_NU];
+  float mu, la;
+  lame(E, nu, mu, la);
+  const float ks = prm[PRM_KS], kc = prm[PRM_KC];
+  float gsum[4] = {0.f, 0.f, 0.f, 0.f};
+  if (valid) {
+    TriGeom g;
+    load_tri(B, Si, t, true, g);
+    Sten st;
+    make_stencil(g.xc, I, st, B.status, ch.inst);
+    float C[9], d3[3], Di[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) C[q] = __ldg(Si.t + q * nt + t);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) d3[q] = __ldg(Si.t + (9 + q) * nt + t);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) Di[q] = __ldg(rest + q * nt + t);
+    M3<float> d, F;
+    tri_F(g, d3, Di, d, F);
+    Stress<float> sts;
+    stress_forward<float>(F, mu, la, ks, kc, sts);
+    const float vol = I.vol_q, dt = B.dt, m = I.m_q, dx = I.dx, inv_dx = I.inv_dx;
+    const float cn = -vol * dt;
+    const float P3[3] = {sts.P.m[2], sts.P.m[5], sts.P.m[8]};
+    float sp[3] = {0.f, 0.f, 0.f}, spd[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float bP3[3] = {0.f, 0.f, 0.f}, bd3[3] = {0.f, 0.f, 0.f}, bx[3] = {0.f, 0.f, 0.f};
+    const float mv[3] = {m * g.vc[0], m * g.vc[1], m * g.vc[2]};
+    const float i2 = inv_dx * inv_dx;
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+      const int oi = q / 9, oj = (q / 3) % 3, ok = q % 3;
+      const float w0 = st.w[0][oi], w1 = st.w[1][oj], w2 = st.w[2][ok];
+      const float e0 = st.dw[0][oi], e1 = st.dw[1][oj], e2 = st.dw[2][ok];
+      const float W = w0 * w1 * w2;
+      const float gW[3] = {e0 * w1 * w2 * inv_dx, w0 * e1 * w2 * inv_dx, w0 * w1 * e2 * inv_dx};
+      const float dd0 = bspline_dd<float>(oi), dd1 = bspline_dd<float>(oj), dd2 = bspline_dd<float>(ok);
+      const float H[9] = {dd0 * w1 * w2 * i2, e0 * e1 * w2 * i2, e0 * w1 * e2 * i2,
+                          e0 * e1 * w2 * i2, w0 * dd1 * w2 * i2, w0 * e1 * e2 * i2,
+                          e0 * w1 * e2 * i2, w0 * e1 * e2 * i2, w0 * w1 * dd2 * i2};
+      const float dp[3] = {((float)oi - st.fx[0]) * dx, ((float)oj - st.fx[1]) * dx, ((float)ok - st.fx[2]) * dx};
+      const float4 ga = gadj(B, I, st.base[0] + oi, st.base[1] + oj, st.base[2] + ok);
+      const float bp[3] = {ga.x, ga.y, ga.z};
+      const float gdot = gW[0] * d3[0] + gW[1] * d3[1] + gW[2] * d3[2];
+      const float sP = bp[0] * P3[0] + bp[1] * P3[1] + bp[2] * P3[2];
+      float s = ga.w * m;
+      float ctb[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const float pay = mv[a] + m * (C[3 * a] * dp[0] + C[3 * a + 1] * dp[1] + C[3 * a + 2] * dp[2]);
+        s += bp[a] * pay;
+        sp[a] += W * bp[a];
+        bP3[a] += cn * gdot * bp[a];
+        bd3[a] += cn * sP * gW[a];
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          spd[3 * a + b] += W * bp[a] * dp[b];
+          ctb[b] += C[3 * a + b] * bp[a];
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const float hd = H[3 * b] * d3[0] + H[3 * b + 1] * d3[1] + H[3 * b + 2] * d3[2];
+        bx[b] += s * gW[b] - W * m * ctb[b] + cn * sP * hd;
+      }
+    }
+    // in-plane corner forces: f1 = k P (r1 + r2), f2 = -k P r1, f3 = -k P r2
+    const float kf = vol * dt;
+    float bf[3][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int a = 0; a < 3; ++a) bf[c][a] = B.barf[a * (long long)B.nv + g.vid[c]];
+    const float r1[3] = {Di[0], d.m[1], d.m[2]};
+    const float r2[3] = {Di[3], d.m[4], d.m[5]};
+    M3<float> bP;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+        bP.m[3 * a + b] = kf * (bf[0][a] * (r1[b] + r2[b]) - bf[1][a] * r1[b] - bf[2][a] * r2[b]);
+    bP.m[2] += bP3[0]; bP.m[5] += bP3[1]; bP.m[8] += bP3[2];
+    float br1[3], br2[3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      br1[b] = kf * (sts.P.m[b] * (bf[0][0] - bf[1][0]) + sts.P.m[3 + b] * (bf[0][1] - bf[1][1]) +
+                     sts.P.m[6 + b] * (bf[0][2] - bf[1][2]));
+      br2[b] = kf * (sts.P.m[b] * (bf[0][0] - bf[2][0]) + sts.P.m[3 + b] * (bf[0][1] - bf[2][1]) +
+                     sts.P.m[6 + b] * (bf[0][2] - bf[2][2]));
+    }
+    M3<float> bF;
+    float gmu = 0.f, gla = 0.f, gks = 0.f, gkc = 0.f;
+    stress_backward<float>(sts, mu, la, ks, kc, bP, B.svd_grad, bF, gmu, gla, gks, gkc);
+    // dL/dd = dL/dF D0^-T plus the direct uses of d in r1, r2 and the normal force
+    float bd[9];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+        bd[3 * r + k] = bF.m[3 * r] * Di[3 * k] + bF.m[3 * r + 1] * Di[3 * k + 1] + bF.m[3 * r + 2] * Di[3 * k + 2];
+    bd[1] += br1[1];  // d[0,1]
+    bd[2] += br1[2];  // d[0,2]
+    bd[4] += br2[1];  // d[1,1]
+    bd[5] += br2[2];  // d[1,2]
+    const float be1[3] = {bd[0], bd[3], bd[6]};
+    const float be2[3] = {bd[1], bd[4], bd[7]};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) bd3[a] += bd[3 * a + 2];
+    const float third = 1.f / 3.f;
+    float bxt[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) bxt[a] = third * (bx[a] + B.tri_tmp[a * nt + t]);
+    const long long e3 = 3 * nt;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      B.contrib[a * e3 + 0 * nt + t] = bxt[a] - be1[a] - be2[a];
+      B.contrib[a * e3 + 1 * nt + t] = bxt[a] + be1[a];
+      B.contrib[a * e3 + 2 * nt + t] = bxt[a] + be2[a];
+      const float bvc = third * m * sp[a];
+      B.contrib[(3 + a) * e3 + 0 * nt + t] = bvc;
+      B.contrib[(3 + a) * e3 + 1 * nt + t] = bvc;
+      B.contrib[(3 + a) * e3 + 2 * nt + t] = bvc;
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) Ai.t[q * nt + t] = m * spd[q];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) Ai.t[(9 + a) * nt + t] += bd3[a];
+    // (mu, la) -> (E, nu)
+    const float dmu_dE = 1.f / (2.f * (1.f + nu)), dmu_dnu = -E / (2.f * (1.f + nu) * (1.f + nu));
+    const float D = (1.f + nu) * (1.f - 2.f * nu);
+    const float dla_dE = nu / D, dla_dnu = E * (1.f + 2.f * nu * nu) / (D * D);
+    gsum[0] = gmu * dmu_dE + gla * dla_dE;
+    gsum[1] = gmu * dmu_dnu + gla * dla_dnu;
+    gsum[2] = gks;
+    gsum[3] = gkc;
+  }
+  block_sum_atomic<4>(gsum, gparams + ch.inst * PRM_STRIDE);
+}
+
+__global__ void k_vertex_collect(BatchDev B, float* __restrict__ ain) {
+  StateP Ai = state_ptrs(ain, B.nv, B.nt, B.no);
+  const long long e3 = 3LL * B.nt, nv = B.nv;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nv; v += (long long)gridDim.x * blockDim.x) {
+    float s[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const int e0 = __ldg(B.inc_ptr + v), e1 = __ldg(B.inc_ptr + v + 1);
+    for (int e = e0; e < e1; ++e) {
+      const int id = __ldg(B.inc_e + e);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) s[q] += B.contrib[q * e3 + id];
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      Ai.v[a * nv + v] += s[a];
+      Ai.v[(3 + a) * nv + v] += s[3 + a];
+    }
+  }
+}
+
+// ============================================================== Chamfer
+// compute_loss (parameter_fitting_functions.py:3-15): for every target point
+// the minimum over vertices of |x - t|^2 / 3, evaluated with the reference's
+// float32 operation order; ties go to the vertex of lowest rank.
+__global__ void __launch_bounds__(128) k_chamfer_fwd(BatchDev B, const float* __restrict__ state,
+                                                     const float* __restrict__ targets, int* __restrict__ qarg) {
+  __shared__ float sx[256], sy[256], sz[256];
+  __shared__ int sr[256];
+  const int inst = blockIdx.y;
+  const InstDev& I = B.inst[inst];
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (blockIdx.x * blockDim.x >= I.nq) return;
+  const bool valid = q < I.nq;
+  const long long nq = B.nq, nv = B.nv;
+  const long long gq = (long long)I.q_off + q;
+  float tx = 0.f, ty = 0.f, tz = 0.f;
+  if (valid) {
+    tx = __ldg(targets + gq);
+    ty = __ldg(targets + nq + gq);
+    tz = __ldg(targets + 2 * nq + gq);
+  }
+  float best = __int_as_float(0x7f800000);
+  int brank = 0x7fffffff, bv = -1;
+  for (int base = 0; base < I.nv; base += 256) {
+    for (int j = threadIdx.x; j < 256; j += blockDim.x) {
+      const int v = base + j;
+      if (v < I.nv) {
+        const long long gv = I.v_off + v;
+        sx[j] = __ldg(state + gv);
+        sy[j] = __ldg(state + nv + gv);
+        sz[j] = __ldg(state + 2 * nv + gv);
+        sr[j] = __ldg(B.vertex_rank + gv);
+      }
+    }
+    __syncthreads();
+    const int cnt = min(256, I.nv - base);
+    if (valid) {
+      for (int j = 0; j < cnt; ++j) {
+        const float dx = __fsub_rn(sx[j], tx), dy = __fsub_rn(sy[j], ty), dz = __fsub_rn(sz[j], tz);
+        const float dd = __fdiv_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)), 3.f);
+        if (dd < best || (dd == best && sr[j] < brank)) {
+          best = dd;
+          brank = sr[j];
+          bv = base + j;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (valid) {
+    B.qmin[gq] = bv >= 0 ? best : 0.f;
+    qarg[gq] = bv >= 0 ? I.v_off + bv : -1;
+  }
+}
+
+__global__ void k_chamfer_loss(BatchDev B, float* __restrict__ loss) {
+  __shared__ double red[32];
+  const InstDev& I = B.inst[blockIdx.x];
+  double s = 0.0;
+  for (int q = threadIdx.x; q < I.nq; q += blockDim.x) s += (double)(B.qmin[I.q_off + q] / (float)I.nq);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    loss[blockIdx.x] = (float)t;
+  }
+}
+
+__global__ void k_chamfer_bwd(BatchDev B, const float* __restrict__ state, const float* __restrict__ targets,
+                              const int* __restrict__ qarg, const float* __restrict__ gloss, float* __restrict__ adj) {
+  const int inst = blockIdx.y;
+  const InstDev& I = B.inst[inst];
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= I.nq) return;
+  const long long nq = B.nq, nv = B.nv;
+  const long long gq = (long long)I.q_off + q;
+  const int v = qarg[gq];
+  if (v < 0) return;
+  const float s = __ldg(gloss + inst) / (float)I.nq * (2.f / 3.f);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float d = __ldg(state + a * nv + v) - __ldg(targets + a * nq + gq);
+    atomicAdd(adj + a * nv + v, s * d);
+  }
+}
+
+// ============================================================== launchers
+static inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+cudaError_t launch_init(const BatchDev& B, const float* x0v, const float* x0o, const float* x0c, float* state, float* rest,
+                        cudaStream_t s) {
+  const long long total = (long long)B.nv + B.no + B.nc + B.nt;
+  const int grid = total > 0 ? (ceil_div(total, 256) < 148 * 16 ? ceil_div(total, 256) : 148 * 16) : 1;
+  k_init<<<grid, 256, 0, s>>>(B, x0v, x0o, x0c, state, rest);
+  return cudaGetLastError();
+}
+
+static inline size_t tile_bytes(const BatchDev& B) { return (size_t)B.tile_nodes * sizeof(float4); }
+
+cudaError_t launch_forward(const BatchDev& B, const LaunchCfg& L, const float* params, const float* traj, const float* rest,
+                           int step, int window, const float* sin, float* sout, cudaStream_t s) {
+  cudaMemsetAsync(B.counters, 0, sizeof(int), s);
+  if (B.n_tri_chunks) k_tri_forward<<<B.n_tri_chunks, L.block, tile_bytes(B), s>>>(B, params, rest, sin);
+  if (B.n_point_chunks) k_point_p2g<<<B.n_point_chunks, L.block, tile_bytes(B), s>>>(B, traj, step, window, sin);
+  k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_FORWARD);
+  k_g2p<<<B.n_tri_chunks + B.n_point_chunks, L.block, 0, s>>>(B, params, sin, sout);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_backward(const BatchDev& B, const LaunchCfg& L, const float* params, const float* traj,
+                            const float* rest, int step, int window, const float* sin, const float* aout, float* ain,
+                            double* gparams, double* gtraj, cudaStream_t s) {
+  cudaMemsetAsync(B.counters, 0, sizeof(int), s);
+  if (B.n_tri_chunks) k_tri_forward<<<B.n_tri_chunks, L.block, tile_bytes(B), s>>>(B, params, rest, sin);
+  if (B.n_point_chunks) k_point_p2g<<<B.n_point_chunks, L.block, tile_bytes(B), s>>>(B, traj, step, window, sin);
+  k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_RECOMPUTE);
+  k_g2p_adj<<<B.n_tri_chunks + B.n_point_chunks, L.block, tile_bytes(B), s>>>(B, params, sin, aout, ain, gparams);
+  k_grid_adj<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, gparams, gtraj);
+  if (B.n_point_chunks) k_point_adj<<<B.n_point_chunks, L.block, 0, s>>>(B, traj, step, window, sin, ain, gtraj);
+  if (B.n_tri_chunks) k_tri_adj<<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin, ain, gparams);
+  if (B.nv) k_vertex_collect<<<ceil_div(B.nv, 256), 256, 0, s>>>(B, ain);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_chamfer_forward(const BatchDev& B, int max_nq, const float* state, const float* targets, int* qarg,
+                                   float* loss, cudaStream_t s) {
+  if (max_nq > 0) {
+    dim3 grid(ceil_div(max_nq, 128), B.n_inst);
+    k_chamfer_fwd<<<grid, 128, 0, s>>>(B, state, targets, qarg);
+  }
+  k_chamfer_loss<<<B.n_inst, 256, 0, s>>>(B, loss);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_chamfer_backward(const BatchDev& B, int max_nq, const float* state, const float* targets,
+                                    const int* qarg, const float* gloss, float* adj, cudaStream_t s) {
+  if (max_nq > 0) {
+    dim3 grid(ceil_div(max_nq, 128), B.n_inst);
+    k_chamfer_bwd<<<grid, 128, 0, s>>>(B, state, targets, qarg, gloss, adj);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t configure_kernels(const BatchDev& B) {
+  const int bytes = (int)tile_bytes(B);
+  cudaError_t e = cudaSuccess;
+  if (bytes > 48 * 1024) {
+    e = cudaFuncSetAttribute(k_tri_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_point_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_g2p_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  }
+  return e;
+}
+
+}  // namespace dcp

@@ -1,0 +1,264 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and with the
+golden vectors of the reference source.  Needs a B200."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from tests.scenes import oracle_loss, oracle_params, reference_small_scene, small_sheet
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+
+
+def _batch(scenes, **kw):
+    from diffcp_b200.batch import ClothBatch
+    return ClothBatch(scenes, dt=scenes[0].meta["dt"], **kw)
+
+
+def unpack(b, state, i=0):
+    """Fields of instance i in the scene's original particle order (numpy)."""
+    f = b.state_fields(state)
+    vp, tp = b.vperm[i], b.tperm[i]
+    va, vb = int(b.v_off[i]), int(b.v_off[i + 1])
+    ta, tb = int(b.t_off[i]), int(b.t_off[i + 1])
+
+    def vert(x, k):
+        a = x[:, va:vb].t().cpu().numpy().reshape(-1, *k)
+        out = np.empty_like(a)
+        out[vp] = a
+        return out
+
+    def tri(x, k):
+        a = x[:, ta:tb].t().cpu().numpy().reshape(-1, *k)
+        out = np.empty_like(a)
+        out[tp] = a
+        return out
+
+    out = {"vx": vert(f["vx"], (3,)), "vv": vert(f["vv"], (3,)), "vC": vert(f["vC"], (3, 3)),
+           "qC": tri(f["qC"], (3, 3)), "qd3": tri(f["qd3"], (3,))}
+    for k in ("ox", "ov", "cx", "cv"):
+        out[k] = f[k].t().cpu().numpy()
+    out["oC"] = f["oC"].t().cpu().numpy().reshape(-1, 3, 3)
+    out["cC"] = f["cC"].t().cpu().numpy().reshape(-1, 3, 3)
+    return out
+
+
+def oracle_np(st):
+    o = {k: v.detach().numpy() for k, v in st.items()}
+    o["qd3"] = o["qd"][..., 2]
+    return o
+
+
+def rel_err(got, ref):
+    scale = max(float(np.abs(ref).max()), 1e-12)
+    return float(np.abs(got - ref).max()) / scale
+
+
+FIELDS = ("vx", "vv", "vC", "qC", "qd3", "ox", "ov", "oC", "cx", "cv", "cC")
+
+
+@pytest.mark.parametrize("window", [0, 1])
+def test_forward_substeps_match_oracle(window):
+    sc = reference_small_scene()
+    n = sc.meta["max_steps"] - 1
+    _, _, _, _, states = oracle_loss(sc, n, n, window=window)
+    b = _batch([sc])
+    s = b.init_state()
+    worst = {}
+    for f in range(n):
+        s = b.forward_step(s, f, window)
+        got = unpack(b, s)
+        ref = oracle_np(states[f + 1])
+        for k in FIELDS:
+            if ref[k].size:
+                worst[k] = max(worst.get(k, 0.0), rel_err(got[k], ref[k]))
+    assert b.status()[0] & 3 == 0
+    for k, e in worst.items():
+        assert e < 2e-4, (k, e, worst)
+
+
+def test_forward_matches_reference_source_golden():
+    g = np.load(os.path.join(GOLD, "ref_forward_f32.npz"))
+    sc = reference_small_scene()
+    n = sc.meta["max_steps"] - 1
+    b = _batch([sc])
+    s = b.init_state()
+    names = {"vx": "vertex_x", "vv": "vertex_v", "vC": "vertex_C", "qC": "quadrature_C", "ox": "operator_x",
+             "ov": "operator_v", "oC": "operator_C", "cx": "cube_x", "cv": "cube_v", "cC": "cube_C"}
+    worst = {}
+    for f in range(n):
+        s = b.forward_step(s, f, 0)
+        got = unpack(b, s)
+        for k, name in names.items():
+            ref = g["w0_" + name][f + 1]
+            worst[k] = max(worst.get(k, 0.0), rel_err(got[k], ref))
+        worst["qd3"] = max(worst.get("qd3", 0.0), rel_err(got["qd3"], g["w0_quadrature_d"][f + 1][..., 2]))
+    for k, e in worst.items():
+        assert e < 2e-4, (k, e, worst)
+
+
+@pytest.mark.parametrize("svd_grad", ["exact", "reference"])
+def test_reference_scene_loss_and_gradients(svd_grad):
+    from diffcp_b200.batch import BatchSim
+    sc = reference_small_scene()
+    n = sc.meta["max_steps"] - 1
+    L = n - 2   # compute_loss(f) reads vertex_x[f - 1] after the loop (parameter_fitting_functions.py:7,27-29)
+    b = _batch([sc], svd_grad=svd_grad)
+    sim = BatchSim(b, n_steps=n, loss_step=L, ckpt_every=4)
+    params = b.params.clone().requires_grad_(True)
+    traj = b.traj.clone().requires_grad_(True)
+    loss = sim.loss(params, traj)
+    loss.sum().backward()
+    p = oracle_params(sc, requires_grad=True)
+    seq = torch.tensor(sc.keyframes, dtype=torch.float64, requires_grad=True)
+    lo, p, seq, _, _ = oracle_loss(sc, n, L, params=p, seq=seq, svd_grad=svd_grad)
+    lo.backward()
+    assert float(loss[0]) == pytest.approx(float(lo), rel=1e-5)
+    got = params.grad[0].double().cpu().numpy()
+    ref = [p[k].grad for k in ("E", "nu", "ks", "kc")]
+    for j, r in enumerate(ref):
+        r = float(r)
+        assert abs(got[j] - r) <= 1e-4 * abs(r) + 1e-12, (j, got[j], r)
+    gs = traj.grad.double().cpu().numpy().reshape(seq.shape)
+    rs = seq.grad.numpy()
+    assert np.abs(gs - rs).max() <= 1e-4 * np.abs(rs).max() + 1e-12, (np.abs(gs - rs).max(), np.abs(rs).max())
+
+
+def _sheet_grads(sc, n, b=None, ckpt_every=5, **kw):
+    from diffcp_b200.batch import BatchSim
+    b = b or _batch([sc], **kw)
+    sim = BatchSim(b, n_steps=n, loss_step=n, ckpt_every=ckpt_every)
+    params = b.params.clone().requires_grad_(True)
+    traj = b.traj.clone().requires_grad_(True)
+    loss = sim.loss(params, traj)
+    loss.sum().backward()
+    return loss.detach(), params.grad.double().cpu().numpy(), traj.grad.double().cpu().numpy(), b
+
+
+def test_kinematic_sheet_loss_and_gradients():
+    n = 30
+    sc = small_sheet(n_steps=n)
+    loss, gp, gt, b = _sheet_grads(sc, n)
+    p = oracle_params(sc, requires_grad=True)
+    vel = torch.tensor(sc.velocities, dtype=torch.float64, requires_grad=True)
+    lo, p, _, vel, _ = oracle_loss(sc, n, n, params=p, vel=vel)
+    lo.backward()
+    assert float(loss[0]) == pytest.approx(float(lo), rel=1e-5)
+    for j, k in enumerate(("E", "nu", "ks", "kc", "friction", "damping")):
+        r = float(p[k].grad)
+        assert abs(gp[0, j] - r) <= 1e-4 * abs(r) + 1e-14, (k, gp[0, j], r)
+    gv = gt[: sc.velocities.size].reshape(sc.velocities.shape)
+    rv = vel.grad.numpy()
+    assert np.abs(gv - rv).max() <= 1e-4 * np.abs(rv).max() + 1e-14
+
+
+def test_batched_equals_single_instances():
+    n = 20
+    scenes = [small_sheet(n=5, seed=1, n_steps=n), small_sheet(n=7, seed=2, n_steps=n, E=8e3),
+              small_sheet(n=6, seed=3, n_grid=32, n_steps=n, friction=0.1)]
+    lb, gpb, gtb, bb = _sheet_grads(None, n, b=_batch(scenes))
+    for i, sc in enumerate(scenes):
+        l1, gp1, gt1, _ = _sheet_grads(sc, n)
+        assert float(lb[i]) == pytest.approx(float(l1[0]), rel=1e-5)
+        np.testing.assert_allclose(gpb[i, :6], gp1[0, :6], rtol=1e-4, atol=1e-14)
+        off, ln = bb.traj_slices(i)
+        np.testing.assert_allclose(gtb[off: off + ln // 2], gt1[: ln // 2], rtol=1e-4,
+                                   atol=1e-4 * np.abs(gt1).max() + 1e-14)
+
+
+@pytest.mark.parametrize("K", [1, 3, 30])
+def test_checkpoint_interval_does_not_change_gradients(K):
+    from diffcp_b200.batch import BatchSim
+    n = 24
+    sc = small_sheet(n_steps=n)
+    res = []
+    for kk in (K, 24):
+        b = _batch([sc])
+        sim = BatchSim(b, n_steps=n, ckpt_every=kk)
+        params = b.params.clone().requires_grad_(True)
+        traj = b.traj.clone().requires_grad_(True)
+        sim.loss(params, traj).sum().backward()
+        res.append((params.grad.double().cpu().numpy(), traj.grad.double().cpu().numpy()))
+    np.testing.assert_allclose(res[0][0], res[1][0], rtol=1e-5, atol=1e-16)
+    np.testing.assert_allclose(res[0][1], res[1][1], rtol=1e-5, atol=1e-5 * np.abs(res[1][1]).max())
+
+
+def test_graph_replay_equals_eager():
+    from diffcp_b200.batch import BatchSim
+    n = 16
+    sc = small_sheet(n_steps=n)
+    out = []
+    for g in (False, True, True):
+        b = _batch([sc])
+        sim = BatchSim(b, n_steps=n, ckpt_every=4, use_graph=g)
+        params = b.params.clone().requires_grad_(True)
+        traj = b.traj.clone().requires_grad_(True)
+        loss = sim.loss(params, traj)
+        loss.sum().backward()
+        out.append((loss.detach().cpu().numpy(), params.grad.cpu().numpy()))
+    for o in out[1:]:
+        np.testing.assert_allclose(o[0], out[0][0], rtol=1e-6)
+        np.testing.assert_allclose(o[1], out[0][1], rtol=1e-5, atol=1e-16)
+
+
+def test_tile_fallback_path_matches_tiled_path():
+    n = 12
+    sc = small_sheet(n_steps=n)
+    l1, g1, t1, _ = _sheet_grads(sc, n)
+    l2, g2, t2, b2 = _sheet_grads(sc, n, b=_batch([sc], tile_nodes=0))
+    assert float(l1[0]) == pytest.approx(float(l2[0]), rel=1e-6)
+    np.testing.assert_allclose(g1, g2, rtol=1e-5, atol=1e-16)
+
+
+def test_chamfer_forward_argmin_and_backward():
+    rng = np.random.default_rng(0)
+    scenes = [small_sheet(n=6, seed=5), small_sheet(n=8, seed=6)]
+    for sc in scenes:
+        sc.targets = sc.vertices[rng.choice(sc.n_vertex, 40)] + rng.normal(0, 0.01, (40, 3))
+        sc.targets[:3] = sc.vertices[:3]          # exact hits
+    b = _batch(scenes)
+    s = b.init_state()
+    loss, arg = b.chamfer(s)
+    torch.cuda.synchronize()
+    for i, sc in enumerate(scenes):
+        x = sc.vertices.astype(np.float32)
+        t = sc.targets.astype(np.float32)
+        d = (x[:, None, :] - t[None, :, :])
+        sq = d * d
+        dist = ((sq[..., 0] + sq[..., 1]) + sq[..., 2]) / np.float32(3)
+        ref_arg = dist.argmin(0)
+        a, bq = int(b.q_off[i]), int(b.q_off[i + 1])
+        got = arg[a:bq].cpu().numpy() - int(b.v_off[i])
+        got_orig = b.vperm[i][got]
+        np.testing.assert_array_equal(got_orig, ref_arg)
+        assert float(loss[i]) == pytest.approx(float(dist.min(0).astype(np.float64).mean()), rel=1e-6)
+    gl = torch.ones(len(scenes), device=b.device)
+    adj = torch.zeros(b.S, device=b.device)
+    b.chamfer_backward(s, arg, gl, adj)
+    for i, sc in enumerate(scenes):
+        x = torch.tensor(sc.vertices, dtype=torch.float64, requires_grad=True)
+        from oracle.sim64 import compute_loss
+        lo, _ = compute_loss(x, torch.tensor(sc.targets, dtype=torch.float64))
+        lo.backward()
+        got = b.vertex_x(adj, i).cpu().numpy()
+        np.testing.assert_allclose(got, x.grad.numpy(), rtol=1e-4, atol=1e-4 * np.abs(x.grad.numpy()).max())
+
+
+def test_out_of_domain_particle_sets_status_and_stays_in_bounds():
+    sc = small_sheet(n=5)
+    sc.vertices = sc.vertices.copy()
+    sc.vertices[0] = [0.999, 0.5, 0.5]
+    b = _batch([sc])
+    s = b.init_state()
+    s = b.forward_step(s, 0)
+    st = b.status()
+    assert st[0] & 1
