@@ -1,0 +1,412 @@
+"""Benchmark: fwd+bwd particle-steps/s of the batched differentiable cloth MPM.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload sweep|single|small] [--impl ours|reference]
+
+Workloads (synthetic data; seeded):
+  sweep   256 square cloths, side U{16..96} vertices at the 0.2 m / 31 spacing of
+          the single-cloth case, E log-U[1e3, 1e5], nu U[0.1, 0.45], ground
+          friction U[0.1, 0.6], own 2-corner cubic-spline grasp each, separate
+          64^3 grids, dt 1e-4, 300 substeps, Chamfer to 2048 targets each,
+          gradients of every instance in one pass                   (default)
+          (dt is not fixed by the configuration; 1e-4 keeps the stiffest draw,
+          2mu + lambda ~ 3.8e5 Pa, inside the explicit stability limit, which
+          2e-4 does not)
+  single  one 128x128-vertex cloth, 0.4 m, 128^3 grid, dt 1e-4, 1000 substeps,
+          checkpoints every 50 substeps
+  small   one 32x32-vertex cloth, 0.2 m, 64^3 grid, dt 2e-4, 200 substeps
+
+A step is one forward rollout + Chamfer loss + full adjoint rollout.  Targets are
+area-uniform samples of each cloth's rest surface (no dataset is involved).
+Under torchrun every rank runs its own, differently seeded copy of the workload
+(instances are independent: no collective on the data path) and the line
+reports the whole-job rate from the slowest rank's device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+bwd particle-steps/s"
+UNIT = "particle-steps/s"
+SPACING = 0.2 / 31
+# Algorithmic bytes per particle of one launch (float32 state, grid traffic
+# excluded), for each kernel of the substep and its adjoint; see DESIGN.md.
+KERNEL_BYTES = {
+    "k_tri_forward": {"tri": 252},
+    "k_point_p2g": {"vertex": 72, "corner": 16},
+    "k_grid": {"node": 48},
+    "k_g2p": {"vertex": 84, "tri": 156},
+    "k_g2p_adj": {"vertex": 96, "tri": 180},
+    "k_grid_adj": {"node": 64},
+    "k_point_adj": {"vertex": 144, "corner": 16},
+    "k_tri_adj": {"tri": 396},
+    "k_vertex_collect": {"vertex": 48, "corner": 28},
+}
+# Whole fwd+bwd substep, per particle (float32): vertex 420 B, triangle 1068 B.
+STEP_BYTES = {"vertex": 420, "tri": 1068}
+
+
+def workload(name, seed):
+    from diffcp_b200 import scene
+    if name == "sweep":
+        rng = np.random.default_rng(seed)
+        scenes = []
+        for i in range(256):
+            n = int(rng.integers(16, 97))
+            E = float(10 ** rng.uniform(3, 5))
+            nu = float(rng.uniform(0.1, 0.45))
+            fr = float(rng.uniform(0.1, 0.6))
+            scenes.append(scene.sheet_scene(n=n, side=(n - 1) * SPACING, height=0.3, n_grid=64, dt=1e-4,
+                                            n_steps=300, E=E, nu=nu, friction=fr, seed=seed * 1000 + i,
+                                            n_targets=2048))
+        return scenes, dict(dt=1e-4, n_steps=300, ckpt_every=1,
+                            desc="batched parameter sweep: 256 cloths, side U{16..96} vertices, 64^3 grid each, "
+                                 "dt 1e-4, 300 substeps, Chamfer to 2048 targets each")
+    if name == "single":
+        return [scene.sheet_scene(n=128, side=0.4, height=0.3, n_grid=128, dt=1e-4, n_steps=1000, seed=seed,
+                                  n_targets=2048)], dict(
+            dt=1e-4, n_steps=1000, ckpt_every=50,
+            desc="single cloth 128x128 vertices, 0.4 m, 128^3 grid, dt 1e-4, 1000 substeps, checkpoints every 50")
+    if name == "small":
+        return [scene.sheet_scene(n=32, side=0.2, height=0.3, n_grid=64, dt=2e-4, n_steps=200, seed=seed,
+                                  n_targets=2048)], dict(
+            dt=2e-4, n_steps=200, ckpt_every=1,
+            desc="single cloth 32x32 vertices, 0.2 m, 64^3 grid, dt 2e-4, 200 substeps")
+    raise ValueError(name)
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel, units):
+    """DRAM bytes per particle of ``kernel`` from the committed ncu summary
+    (profiles/<kernel>.md, line 'dram_bytes_per_particle: X'), scaled to a
+    launch of ``units`` particles; None when no summary exists."""
+    path = os.path.join(ROOT, "profiles", kernel + ".md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"dram_bytes_per_particle:\s*([0-9.eE+-]+)", open(path).read())
+    return float(m.group(1)) * units if m else None
+
+
+def counts(scenes):
+    nv = sum(s.n_vertex for s in scenes)
+    nt = sum(s.n_tri for s in scenes)
+    return nv, nt
+
+
+# ------------------------------------------------------------------ CPU
+def cpu_rate(scenes, info, seconds=15.0):
+    """Oracle (torch, float32, all host threads) fwd+bwd rate on a bounded
+    sample of the workload: the instance nearest the median size, as many
+    substeps as fit in about ``seconds``."""
+    import torch
+    from oracle import sim64
+    from oracle.sim64 import Constants, KinematicGripper, OracleSim
+    sizes = [s.n_vertex + s.n_tri for s in scenes]
+    sc = scenes[int(np.argsort(sizes)[len(sizes) // 2])]
+    dt = info["dt"]
+    d = torch.float32
+    const = Constants(n_grid=sc.n_grid, dt=dt, vertex_p_mass=sc.vertex_p_mass, quadrature_p_mass=sc.quadrature_p_mass,
+                      quadrature_p_vol=sc.quadrature_p_vol, gravity_dv=sc.gravity_dv, bound=sc.bound)
+
+    def run(n):
+        osim, st = OracleSim.initialize(const, sc.vertices, sc.triangles, dtype=d)
+        p = {k: torch.tensor(float(v), dtype=d, requires_grad=True) for k, v in
+             zip(("E", "nu", "ks", "kc", "friction", "damping"), sc.param_row())}
+        vel = torch.tensor(sc.velocities, dtype=d, requires_grad=True)
+        grip = KinematicGripper(sc.gripper_radius, torch.tensor(sc.centers, dtype=d), vel)
+        for f in range(n):
+            st = osim.substep(st, f, 0, p, friction=p["friction"], damping=p["damping"], grip=grip)
+        lo, _ = sim64.compute_loss(st["vx"], torch.tensor(sc.targets, dtype=d))
+        lo.backward()
+
+    t0 = time.perf_counter()
+    run(2)
+    per = (time.perf_counter() - t0) / 2
+    n = int(max(2, min(info["n_steps"], seconds / max(per, 1e-3))))
+    t0 = time.perf_counter()
+    run(n)
+    el = time.perf_counter() - t0
+    rate = (sc.n_vertex + sc.n_tri) * n / el
+    return {"value": rate, "unit": UNIT, "cores": torch.get_num_threads(), "kind": "port",
+            "sample": "CPU oracle (torch float32) fwd+bwd of %d substeps of one %d-vertex/%d-triangle cloth of the "
+                      "workload, %.1f s" % (n, sc.n_vertex, sc.n_tri, el)}
+
+
+def profile_substeps(args):
+    """A few eager substeps and adjoint substeps of the workload on a handful
+    of state buffers (a few GB on the device), for kernel profilers."""
+    import torch
+    from diffcp_b200.batch import ClothBatch
+    scenes, info = workload(args.workload, 0)
+    b = ClothBatch(scenes, dt=info["dt"])
+    n = args.profile_substeps
+    states = [b.init_state()]
+    for f in range(n):
+        states.append(b.forward_step(states[-1], f))
+    gp, gt = b.new_grads()
+    adj = torch.zeros(b.S, device=b.device)
+    loss, arg = b.chamfer(states[-1])
+    b.chamfer_backward(states[-1], arg, torch.ones_like(loss), adj)
+    for f in range(n - 1, -1, -1):
+        adj = b.backward_step(states[f], adj, f, gp, gt)
+    torch.cuda.synchronize()
+    st = b.status()
+    print(json.dumps({"profile_substeps": n, "instances": len(scenes), "finite": bool(torch.isfinite(adj).all()),
+                      "status_nonzero": int((st != 0).sum())}))
+
+
+# ------------------------------------------------------------------ main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "single", "small"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile-substeps", type=int, default=0,
+                    help="run this many eager forward + adjoint substeps of the workload and exit (for ncu)")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        scenes, info = workload(args.workload, 0)
+        cb = cpu_rate(scenes, info, seconds=max(args.cpu_seconds, 5.0))
+        line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+                "config": {"workload": info["desc"]}, "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    if args.profile_substeps:
+        return profile_substeps(args)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    from diffcp_b200.batch import BatchSim, ClothBatch
+
+    scenes, info = workload(args.workload, rank)
+    nv, nt = counts(scenes)
+    batch = ClothBatch(scenes, dt=info["dt"], device=dev)
+    sim = BatchSim(batch, n_steps=info["n_steps"], ckpt_every=info["ckpt_every"], use_graph=True)
+    params = batch.params.clone().requires_grad_(True)
+    traj = batch.traj.clone().requires_grad_(True)
+
+    def step():
+        params.grad = None
+        traj.grad = None
+        loss = sim.loss(params, traj)
+        loss.sum().backward()
+        return loss
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(max(args.warmup, 3) if args.warmup >= 0 else 3):
+        step()
+    torch.cuda.synchronize()
+    status = batch.status()
+    launches0 = batch.launch_count()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = (batch.launch_count() - launches0) // max(args.steps, 1)
+    t = torch.tensor([ms], device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(t.item())
+    psteps = (nv + nt) * info["n_steps"]
+    value = psteps * world / (ms_max / 1e3)
+
+    # ---- e2e: public API with host buffers (pinned H2D of the inputs, D2H of loss and gradients)
+    h_params = params.detach().cpu().pin_memory()
+    h_traj = traj.detach().cpu().pin_memory()
+    h_targets = batch.targets.cpu().pin_memory()
+    h_loss = torch.empty(batch.n_inst, dtype=torch.float32).pin_memory()
+    h_gp = torch.empty_like(h_params).pin_memory()
+    h_gt = torch.empty_like(h_traj).pin_memory()
+    d_params = params.detach().clone().requires_grad_(True)
+    d_traj = traj.detach().clone().requires_grad_(True)
+
+    def e2e_step():
+        with torch.no_grad():
+            d_params.copy_(h_params, non_blocking=True)
+            d_traj.copy_(h_traj, non_blocking=True)
+            batch.targets.copy_(h_targets, non_blocking=True)
+        d_params.grad = None
+        d_traj.grad = None
+        loss = sim.loss(d_params, d_traj)
+        loss.sum().backward()
+        h_loss.copy_(loss.detach(), non_blocking=True)
+        h_gp.copy_(d_params.grad, non_blocking=True)
+        h_gt.copy_(d_traj.grad, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1) / args.steps
+    t = torch.tensor([ms_e2e], device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    e2e_val = psteps * world / (float(t.item()) / 1e3)
+    h2d = (h_params.numel() + h_traj.numel() + h_targets.numel()) * 4
+    d2h = (h_loss.numel() + h_gp.numel() + h_gt.numel()) * 4
+
+    # ---- per-kernel device time of one eager step (CUDA events on the launch stream)
+    batch.profile(True)
+    sim.use_graph = False
+    step()
+    torch.cuda.synchronize()
+    prof = batch.profile_read()
+    batch.profile(False)
+    sim.use_graph = True
+    n_nodes_active = None
+    units = {"tri": nt, "vertex": nv, "corner": 3 * nt}
+    dom = max(prof.items(), key=lambda kv: kv[1][0])
+    dname, (dms, dn) = dom
+    per_unit = KERNEL_BYTES.get(dname, {})
+    alg = sum(units.get(u, 0) * b for u, b in per_unit.items())
+    avg_s = dms / dn / 1e3
+    peak, peak_kind = peaks()
+    achieved = alg / avg_s / 1e9 if alg else None
+    traffic = ncu_traffic(dname, units["tri"] if "tri" in per_unit else units["vertex"])
+    roof = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
+            if peak_kind == "measured" else "fallback", "traffic": traffic, "alg_bytes_per_launch": alg,
+            "avg_launch_ms": dms / dn, "launches_in_profile_step": dn}
+    total_prof_ms = sum(v[0] for v in prof.values())
+    step_alg = (nv * STEP_BYTES["vertex"] + nt * STEP_BYTES["tri"]) * info["n_steps"]
+    kernels = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / total_prof_ms, 4)}
+               for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
+
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    cpu = None if args.no_cpu or world > 1 else cpu_rate(scenes, info, seconds=args.cpu_seconds)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": info["desc"], "instances": len(scenes), "vertices": nv, "triangles": nt,
+                   "substeps": info["n_steps"], "checkpoint_every": info["ckpt_every"],
+                   "l2": "inputs larger than L2 (state snapshot %.0f MB, rollout buffer %.1f GB)"
+                         % (batch.S * 4 / 1e6, sim._buf.numel() * 4 / 1e9),
+                   "parallelism": "independent instances per rank" if world > 1 else "one GPU"},
+        "roofline": roof,
+        "step_roofline": {"achieved": step_alg / (ms_max / 1e3) / 1e9, "unit": "GB/s", "peak": peak,
+                          "frac": step_alg / (ms_max / 1e3) / 1e9 / peak,
+                          "bytes_per_particle": STEP_BYTES},
+        "kernels": kernels,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": float(t.item())},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "status_nonzero_instances": int((status != 0).sum()),
+        "nonfinite_instances": int(((status & 2) != 0).sum()),
+    }
+    print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -110,7 +110,7 @@ class ClothBatch:
         self.params = torch.tensor(np.array([sc.param_row() + [0.0, 0.0] for sc in self.scenes]), **f32)
         self.traj = torch.tensor(self.pack_traj(), **f32) if sizes.traj_floats else torch.zeros(1, **f32)
         self.targets = self.pack_targets([sc.targets for sc in self.scenes]) if self.nq else torch.zeros(3, 1, **f32)
-        self.rest = torch.empty(max(9 * self.nt, 1), **f32)
+        self.rest = torch.empty(max(int(sizes.rest_floats), 1), **f32)
 
     # ------------------------------------------------------------- packing
     def pack_traj(self) -> np.ndarray:
@@ -143,16 +143,40 @@ class ClothBatch:
         return torch.tensor(arr.T.copy(), dtype=torch.float32, device=self.device).contiguous()
 
     # ------------------------------------------------------------- views
-    def vertex_x(self, state: torch.Tensor, i: int) -> torch.Tensor:
-        """(Nv_i, 3) positions of instance i in the scene's original order."""
+    def vertex_x(self, state: torch.Tensor, i: int, absolute: bool = True) -> torch.Tensor:
+        """(Nv_i, 3) positions (``absolute``) or displacements / adjoints of
+        instance i in the scene's original order."""
         a, b = int(self.v_off[i]), int(self.v_off[i + 1])
-        x = state[: 3 * self.nv].view(3, self.nv)[:, a:b].t()
+        x = state[: 3 * self.nv].view(3, self.nv)[:, a:b]
+        if absolute:
+            x = x + self.rest_x0()[:, a:b]
+        x = x.t()
         out = torch.empty_like(x)
         out[torch.as_tensor(self.vperm[i], device=x.device)] = x
         return out
 
+    def rest_x0(self) -> torch.Tensor:
+        """[3][Nv] rest vertex positions held in the rest buffer."""
+        o = 12 * self.nt
+        return self.rest[o: o + 3 * self.nv].view(3, self.nv)
+
+    def rest_n0(self) -> torch.Tensor:
+        return self.rest[9 * self.nt: 12 * self.nt].view(3, self.nt)
+
+    def absolute_fields(self, state: torch.Tensor):
+        """Like :meth:`state_fields` with positions and d3 made absolute."""
+        f = dict(self.state_fields(state))
+        o = 12 * self.nt + 3 * self.nv
+        f["vx"] = f["vx"] + self.rest_x0()
+        f["qd3"] = f["qd3"] + self.rest_n0()
+        f["ox"] = f["ox"] + self.rest[o: o + 3 * self.no].view(3, self.no)
+        o += 3 * self.no
+        f["cx"] = f["cx"] + self.rest[o: o + 3 * self.nc].view(3, self.nc)
+        return f
+
     def state_fields(self, state: torch.Tensor):
-        """Dict of component-major views of one state snapshot."""
+        """Dict of component-major views of one state snapshot (positions are
+        displacements from the rest configuration, 'qd3' is d3 - n0)."""
         nv, nt, no, nc = self.nv, self.nt, self.no, self.nc
         v = state[: 15 * nv].view(15, nv)
         t = state[15 * nv: 15 * nv + 12 * nt].view(12, nt)
@@ -194,14 +218,14 @@ class ClothBatch:
         targets = self.targets if targets is None else targets
         loss = torch.empty(self.n_inst, dtype=torch.float32, device=self.device)
         arg = torch.empty(max(self.nq, 1), dtype=torch.int32, device=self.device)
-        check(self.lib.dcp_chamfer_forward(self.handle, _ptr(state), _ptr(targets), _ptr(arg), _ptr(loss), _stream()),
-              "dcp_chamfer_forward")
+        check(self.lib.dcp_chamfer_forward(self.handle, _ptr(self.rest), _ptr(state), _ptr(targets), _ptr(arg),
+                                           _ptr(loss), _stream()), "dcp_chamfer_forward")
         return loss, arg
 
     def chamfer_backward(self, state, argmin, gloss, adj, targets=None):
         targets = self.targets if targets is None else targets
-        check(self.lib.dcp_chamfer_backward(self.handle, _ptr(state), _ptr(targets), _ptr(argmin), _ptr(gloss),
-                                            _ptr(adj), _stream()), "dcp_chamfer_backward")
+        check(self.lib.dcp_chamfer_backward(self.handle, _ptr(self.rest), _ptr(state), _ptr(targets), _ptr(argmin),
+                                            _ptr(gloss), _ptr(adj), _stream()), "dcp_chamfer_backward")
         return adj
 
     def rollout_buffer(self, n_steps: int, ckpt_every: int) -> torch.Tensor:
@@ -226,6 +250,20 @@ class ClothBatch:
                                             n_steps, loss_step, ckpt_every, _ptr(buf), _ptr(adj_work),
                                             _ptr(gparams), _ptr(gtraj), int(use_graph), _stream()),
               "dcp_rollout_backward")
+
+    def launch_count(self) -> int:
+        return int(self.lib.dcp_launch_count(self.handle))
+
+    def profile(self, enable: bool) -> None:
+        check(self.lib.dcp_profile(self.handle, int(enable)), "dcp_profile")
+
+    def profile_read(self):
+        """{kernel name: (total ms, launches)} of the launches since profile(True)."""
+        k = int(self.lib.dcp_kernel_count())
+        ms = (ctypes.c_double * k)()
+        n = (ctypes.c_int64 * k)()
+        check(self.lib.dcp_profile_read(self.handle, ms, n), "dcp_profile_read")
+        return {self.lib.dcp_kernel_name(i).decode(): (ms[i], n[i]) for i in range(k) if n[i]}
 
     def status(self, clear: bool = True) -> np.ndarray:
         out = (ctypes.c_int32 * self.n_inst)()

@@ -150,6 +150,7 @@ struct GraphCache {
   bool valid = false;
   std::vector<long long> key;
   cudaGraphExec_t exec = nullptr;
+  long long launches = 0;  // kernels per replay
 };
 
 struct DcpBatch {
@@ -162,12 +163,13 @@ struct DcpBatch {
   cudaStream_t cap_stream = nullptr;
   cudaEvent_t ev_a = nullptr, ev_b = nullptr;
   GraphCache gfwd, gbwd;
+  Profiler prof;
 };
 
 static void fill_sizes(const Layout& L, int n, DcpSizes* s) {
   s->n_vertex = L.nv; s->n_tri = L.nt; s->n_operator = L.no; s->n_cube = L.nc; s->n_target = L.nq;
   s->state_floats = 15 * (L.nv + L.no + L.nc) + 12 * L.nt;
-  s->rest_floats = 9 * L.nt;
+  s->rest_floats = 12 * L.nt + 3 * (L.nv + L.no + L.nc);
   s->traj_floats = L.traj;
   s->param_floats = (long long)PRM_STRIDE * n;
   s->static_bytes = (long long)L.static_bytes;
@@ -180,6 +182,9 @@ static void fill_sizes(const Layout& L, int n, DcpSizes* s) {
 extern "C" {
 
 const char* dcp_last_error(void) { return g_err.c_str(); }
+
+int32_t dcp_kernel_count(void) { return KID_COUNT; }
+const char* dcp_kernel_name(int32_t id) { return (id >= 0 && id < KID_COUNT) ? kKernelNames[id] : ""; }
 
 int dcp_plan(const DcpInstance* inst, int32_t n_inst, const DcpOptions* opt, DcpSizes* out) {
   int rc = validate(inst, n_inst, opt);
@@ -277,6 +282,7 @@ int dcp_create(const DcpInstance* inst, int32_t n_inst, const DcpOptions* opt, c
   B.total_blocks = L.total_nodes / 64;
   b->L.block = opt->chunk;
   b->L.grid_ctas = opt->grid_ctas > 0 ? opt->grid_ctas : 148 * 8;
+  b->L.prof = &b->prof;
   e = configure_kernels(B);
   if (e != cudaSuccess) {
     delete b;
@@ -299,6 +305,11 @@ int dcp_destroy(DcpBatch* b) {
   if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
   if (b->ev_a) cudaEventDestroy(b->ev_a);
   if (b->ev_b) cudaEventDestroy(b->ev_b);
+  for (auto& r : b->prof.recs) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (auto e : b->prof.pool) cudaEventDestroy(e);
   delete b;
   return DCP_OK;
 }
@@ -307,7 +318,7 @@ int dcp_init_state(DcpBatch* b, const float* x0v, const float* x0o, const float*
                    void* stream) {
   if (!b || !state0 || !rest || (!x0v && b->B.nv) || (!x0o && b->B.no) || (!x0c && b->B.nc))
     return fail(DCP_ERR_INVALID, "NULL argument");
-  cudaError_t e = launch_init(b->B, x0v, x0o, x0c, state0, rest, (cudaStream_t)stream);
+  cudaError_t e = launch_init(b->B, b->L, x0v, x0o, x0c, state0, rest, (cudaStream_t)stream);
   return e == cudaSuccess ? DCP_OK : cuda_fail(e, "dcp_init_state");
 }
 
@@ -330,17 +341,20 @@ int dcp_substep_backward(DcpBatch* b, const float* params, const float* traj, co
   return e == cudaSuccess ? DCP_OK : cuda_fail(e, "dcp_substep_backward");
 }
 
-int dcp_chamfer_forward(DcpBatch* b, const float* state, const float* targets, int32_t* argmin, float* loss,
-                        void* stream) {
-  if (!b || !state || !loss || (b->B.nq && (!targets || !argmin))) return fail(DCP_ERR_INVALID, "NULL argument");
-  cudaError_t e = launch_chamfer_forward(b->B, b->lay.max_nq, state, targets, argmin, loss, (cudaStream_t)stream);
+int dcp_chamfer_forward(DcpBatch* b, const float* rest, const float* state, const float* targets, int32_t* argmin,
+                        float* loss, void* stream) {
+  if (!b || !rest || !state || !loss || (b->B.nq && (!targets || !argmin))) return fail(DCP_ERR_INVALID, "NULL argument");
+  cudaError_t e =
+      launch_chamfer_forward(b->B, b->L, b->lay.max_nq, rest, state, targets, argmin, loss, (cudaStream_t)stream);
   return e == cudaSuccess ? DCP_OK : cuda_fail(e, "dcp_chamfer_forward");
 }
 
-int dcp_chamfer_backward(DcpBatch* b, const float* state, const float* targets, const int32_t* argmin,
-                         const float* gloss, float* adj, void* stream) {
-  if (!b || !state || !gloss || !adj || (b->B.nq && (!targets || !argmin))) return fail(DCP_ERR_INVALID, "NULL argument");
-  cudaError_t e = launch_chamfer_backward(b->B, b->lay.max_nq, state, targets, argmin, gloss, adj, (cudaStream_t)stream);
+int dcp_chamfer_backward(DcpBatch* b, const float* rest, const float* state, const float* targets,
+                         const int32_t* argmin, const float* gloss, float* adj, void* stream) {
+  if (!b || !rest || !state || !gloss || !adj || (b->B.nq && (!targets || !argmin)))
+    return fail(DCP_ERR_INVALID, "NULL argument");
+  cudaError_t e = launch_chamfer_backward(b->B, b->L, b->lay.max_nq, rest, state, targets, argmin, gloss, adj,
+                                          (cudaStream_t)stream);
   return e == cudaSuccess ? DCP_OK : cuda_fail(e, "dcp_chamfer_backward");
 }
 
@@ -373,7 +387,7 @@ template <class F>
 static int run_maybe_graph(DcpBatch* b, GraphCache& gc, const std::vector<long long>& key, int use_graph, void* stream,
                            F&& body) {
   cudaStream_t us = (cudaStream_t)stream;
-  if (!use_graph) {
+  if (!use_graph || b->prof.timing) {  // per-kernel timing needs eager launches
     cudaError_t e = body(us);
     return e == cudaSuccess ? DCP_OK : cuda_fail(e, "rollout");
   }
@@ -393,7 +407,10 @@ static int run_maybe_graph(DcpBatch* b, GraphCache& gc, const std::vector<long l
     gc.valid = false;
     e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_fail(e, "begin capture");
+    const long long before = b->prof.launches;
     cudaError_t eb = body(cs);
+    gc.launches = b->prof.launches - before;
+    b->prof.launches = before;
     cudaGraph_t g = nullptr;
     e = cudaStreamEndCapture(cs, &g);
     if (eb != cudaSuccess) {
@@ -410,6 +427,7 @@ static int run_maybe_graph(DcpBatch* b, GraphCache& gc, const std::vector<long l
   e = cudaEventRecord(b->ev_a, us);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, b->ev_a, 0);
   if (e == cudaSuccess) e = cudaGraphLaunch(gc.exec, cs);
+  b->prof.launches += gc.launches;
   if (e == cudaSuccess) e = cudaEventRecord(b->ev_b, cs);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(us, b->ev_b, 0);
   return e == cudaSuccess ? DCP_OK : cuda_fail(e, "graph launch");
@@ -465,6 +483,37 @@ int dcp_rollout_backward(DcpBatch* b, const float* params, const float* traj, co
     }
     return cudaSuccess;
   });
+}
+
+int64_t dcp_launch_count(const DcpBatch* b) { return b ? b->prof.launches : -1; }
+
+int dcp_profile(DcpBatch* b, int32_t enable) {
+  if (!b) return fail(DCP_ERR_INVALID, "NULL batch");
+  for (auto& r : b->prof.recs) {
+    b->prof.pool.push_back(r.a);
+    b->prof.pool.push_back(r.b);
+  }
+  b->prof.recs.clear();
+  b->prof.timing = enable != 0;
+  return DCP_OK;
+}
+
+int dcp_profile_read(DcpBatch* b, double* total_ms, int64_t* launches) {
+  if (!b || !total_ms || !launches) return fail(DCP_ERR_INVALID, "NULL argument");
+  for (int k = 0; k < KID_COUNT; ++k) {
+    total_ms[k] = 0.0;
+    launches[k] = 0;
+  }
+  for (auto& r : b->prof.recs) {
+    cudaError_t e = cudaEventSynchronize(r.b);
+    if (e != cudaSuccess) return cuda_fail(e, "dcp_profile_read");
+    float ms = 0.f;
+    e = cudaEventElapsedTime(&ms, r.a, r.b);
+    if (e != cudaSuccess) return cuda_fail(e, "dcp_profile_read");
+    total_ms[r.id] += ms;
+    launches[r.id] += 1;
+  }
+  return DCP_OK;
 }
 
 int dcp_read_status(DcpBatch* b, int32_t* host_status, int32_t clear, void* stream) {

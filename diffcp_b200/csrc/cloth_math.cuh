@@ -88,25 +88,44 @@ template <class T> DCP_HD T bspline_dd(int o) { return o == 1 ? T(-2) : T(1); }
 // Classical Gram-Schmidt with norm(eps) = sqrt(|v|^2 + 1e-9) as in
 // simulation.py:123-135.  R = Q^-1 F is the upper-triangular coefficient
 // matrix [[n1, r01, r02], [0, n2, r12], [0, 0, n3]] (exactly, as a function of F).
+//
+// The input is the deviation Ed = F - I.  Cloth strains are small, so the
+// quantities that drive the stress (n_i - 1, J - 1, 1 - R22) would lose most
+// of their float32 digits if formed as differences of O(1) numbers; here they
+// are evaluated from Ed through exact identities instead:
+//   |f1|^2 - 1 = 2 e1.x + |e1|^2,  f2.f1 = e2.x + e1.y + e1.e2, ...
+//   |h2|^2 - 1 = (|f2|^2 - 1) - r01^2 (2 - |q1|^2), and likewise for h3.
 template <class T> struct QR {
   V3<T> f1, f2, f3, q1, q2, q3, h2, h3;
   T n1, n2, n3, r01, r02, r12;
+  T a1, a2, a3;  // n_i - 1
 };
-template <class T> DCP_HD void qr_forward(const M3<T>& F, QR<T>& s) {
+template <class T> DCP_HD void qr_forward(const M3<T>& Ed, QR<T>& s) {
   const T eps = T(1e-9);
-  s.f1 = col(F, 0);
-  s.f2 = col(F, 1);
-  s.f3 = col(F, 2);
-  s.n1 = sqrt(dot(s.f1, s.f1) + eps);
+  const V3<T> e1 = col(Ed, 0), e2 = col(Ed, 1), e3 = col(Ed, 2);
+  s.f1 = v3(T(1) + e1.x, e1.y, e1.z);
+  s.f2 = v3(e2.x, T(1) + e2.y, e2.z);
+  s.f3 = v3(e3.x, e3.y, T(1) + e3.z);
+  const T s1 = T(2) * e1.x + dot(e1, e1);
+  s.n1 = sqrt(T(1) + (s1 + eps));
+  s.a1 = (s1 + eps) / (s.n1 + T(1));
   s.q1 = s.f1 / s.n1;
-  s.r01 = dot(s.f2, s.q1);
+  const T q11 = T(1) - eps / (s.n1 * s.n1);           // |q1|^2
+  s.r01 = (e2.x + e1.y + dot(e1, e2)) / s.n1;         // f2 . q1
   s.h2 = s.f2 - s.r01 * s.q1;
-  s.n2 = sqrt(dot(s.h2, s.h2) + eps);
+  const T t2 = (T(2) * e2.y + dot(e2, e2)) - s.r01 * s.r01 * (T(2) - q11);   // |h2|^2 - 1
+  s.n2 = sqrt(T(1) + (t2 + eps));
+  s.a2 = (t2 + eps) / (s.n2 + T(1));
   s.q2 = s.h2 / s.n2;
-  s.r02 = dot(s.f3, s.q1);
-  s.r12 = dot(s.f3, s.q2);
+  const T q22 = T(1) - eps / (s.n2 * s.n2);           // |q2|^2
+  const T q12 = s.r01 * (T(1) - q11) / s.n2;          // q1 . q2
+  s.r02 = (e3.x + e1.z + dot(e1, e3)) / s.n1;         // f3 . q1
+  s.r12 = ((e3.y + e2.z + dot(e2, e3)) - s.r01 * s.r02) / s.n2;   // f3 . q2
   s.h3 = s.f3 - s.r02 * s.q1 - s.r12 * s.q2;
-  s.n3 = sqrt(dot(s.h3, s.h3) + eps);
+  const T t3 = (T(2) * e3.z + dot(e3, e3)) - s.r02 * s.r02 * (T(2) - q11) - s.r12 * s.r12 * (T(2) - q22) +
+               T(2) * s.r02 * s.r12 * q12;            // |h3|^2 - 1
+  s.n3 = sqrt(T(1) + (t3 + eps));
+  s.a3 = (t3 + eps) / (s.n3 + T(1));
   s.q3 = s.h3 / s.n3;
 }
 // Adjoint of y = h / n with n = sqrt(|h|^2 + eps): returns dL/dh.
@@ -231,7 +250,8 @@ enum SvdGrad { SVD_GRAD_EXACT = 0, SVD_GRAD_REFERENCE = 1 };
 template <class T> struct Stress {
   QR<T> qr;
   T c, s, rr;        // rotation factor Rp = [[c, -s], [s, c]], rr = |(x, y)|
-  T J;
+  T cm1;             // c - 1
+  T J, Jm1;          // det Fh and det Fh - 1
   T Ri[6];           // R^-1 upper triangle: i00 i01 i02 i11 i12 i22
   T A[6];            // symmetric A: a00 a01 a02 a11 a12 a22
   bool contact;      // R22 <= 1
@@ -239,18 +259,20 @@ template <class T> struct Stress {
   M3<T> P;
 };
 
-template <class T> DCP_HD void stress_forward(const M3<T>& F, T mu, T la, T ks, T kc, Stress<T>& st) {
+// ``Ed`` is F - I (see qr_forward).
+template <class T> DCP_HD void stress_forward(const M3<T>& Ed, T mu, T la, T ks, T kc, Stress<T>& st) {
   QR<T>& q = st.qr;
-  qr_forward(F, q);
+  qr_forward(Ed, q);
   const T n1 = q.n1, n2 = q.n2, n3 = q.n3, r01 = q.r01, r02 = q.r02, r12 = q.r12;
+  const T a1 = q.a1, a2 = q.a2, a3 = q.a3;
   // A (simulation.py:215-229); the first write of A[0,0] (line 216) is dead.
-  st.contact = n3 <= T(1);
+  st.contact = a3 <= T(0);
   st.A[0] = ks * r02 * r02;
   st.A[1] = ks * r02 * r12;
   st.A[2] = ks * r02 * n3;
   st.A[3] = ks * r12 * r12;
   st.A[4] = ks * r12 * n3;
-  st.A[5] = st.contact ? (-kc) * ((T(1) - n3) * (T(1) - n3)) * n3 : T(0);
+  st.A[5] = st.contact ? (-kc) * (a3 * a3) * n3 : T(0);
   // R^-1 of the upper-triangular R
   const T i00 = T(1) / n1, i11 = T(1) / n2, i22 = T(1) / n3;
   st.Ri[0] = i00;
@@ -259,17 +281,22 @@ template <class T> DCP_HD void stress_forward(const M3<T>& F, T mu, T la, T ks, 
   st.Ri[3] = i11;
   st.Ri[4] = -r12 * i11 * i22;
   st.Ri[5] = i22;
-  // rotation factor of Fh and J
-  const T x = n1 + n2, y = -r01;
-  st.rr = sqrt(x * x + y * y);
-  st.c = x / st.rr;
-  st.s = y / st.rr;
+  // rotation factor of Fh = [[n1, r01], [0, n2]]: (c, s) = (x, y) / |(x, y)|,
+  // x = n1 + n2 > 0, y = -r01; c - 1 = -tau^2 / (w (1 + w)), tau = y / x.
+  const T x = T(2) + (a1 + a2), y = -r01;
+  const T tau = y / x;
+  const T w = sqrt(T(1) + tau * tau);
+  st.rr = x * w;
+  st.c = T(1) / w;
+  st.s = tau / w;
+  st.cm1 = -(tau * tau) / (w * (T(1) + w));
   st.J = n1 * n2;
-  const T lj = la * (st.J - T(1));
-  const T p00 = T(2) * mu * (n1 - st.c) + lj * n2;
+  st.Jm1 = a1 + a2 + a1 * a2;
+  const T lj = la * st.Jm1;
+  const T p00 = T(2) * mu * (a1 - st.cm1) + lj * n2;
   const T p01 = T(2) * mu * (r01 + st.s);
   const T p10 = T(2) * mu * (-st.s) + lj * (-r01);
-  const T p11 = T(2) * mu * (n2 - st.c) + lj * n1;
+  const T p11 = T(2) * mu * (a2 - st.cm1) + lj * n1;
   // M = pad(P_fc) + A R^-T, (A R^-T)[r][c] = sum_{k>=c} A[r][k] Rinv[c][k]
   const T* a = st.A;
   const T Ar[3][3] = {{a[0], a[1], a[2]}, {a[1], a[3], a[4]}, {a[2], a[4], a[5]}};
@@ -358,14 +385,14 @@ DCP_HD void stress_backward(const Stress<T>& st, T mu, T la, T ks, T kc, const M
   gr12 += ks * (r02 * s01 + T(2) * r12 * gA[1][1] + n3 * s12);
   gn3 += ks * (r02 * s02 + r12 * s12);
   if (st.contact) {
-    const T om = T(1) - n3;
+    const T om = -st.qr.a3;  // 1 - n3
     gn3 += gA[2][2] * (-kc) * (om * om - T(2) * om * n3);
     gkc += gA[2][2] * (-(om * om) * n3);
   }
   // --- fixed-corotated in-plane part
   const T c = st.c, s = st.s;
-  gmu += T(2) * (g00 * (n1 - c) + g01 * (r01 + s) + g10 * (-s) + g11 * (n2 - c));
-  gla += (st.J - T(1)) * (g00 * n2 + g10 * (-r01) + g11 * n1);
+  gmu += T(2) * (g00 * (st.qr.a1 - st.cm1) + g01 * (r01 + s) + g10 * (-s) + g11 * (st.qr.a2 - st.cm1));
+  gla += st.Jm1 * (g00 * n2 + g10 * (-r01) + g11 * n1);
   // direct Fh term
   gn1 += T(2) * mu * g00;
   gr01 += T(2) * mu * g01;
@@ -374,7 +401,7 @@ DCP_HD void stress_backward(const Stress<T>& st, T mu, T la, T ks, T kc, const M
   const T gJ = la * (g00 * n2 + g10 * (-r01) + g11 * n1);
   gn1 += gJ * n2;
   gn2 += gJ * n1;
-  const T lj = la * (st.J - T(1));
+  const T lj = la * st.Jm1;
   gn2 += lj * g00;
   gr01 -= lj * g10;
   gn1 += lj * g11;
@@ -466,13 +493,15 @@ DCP_HD void grid_bc_backward(const T v[3], const NodeBC<T>& r, T mu_g, const T g
   gv[1] = T(0);
   if (r.vt > T(0)) {
     if (r.scale > T(0)) {
-      const T gdot = gout[0] * v[0] + gout[2] * v[2];
-      const T vt = r.vt;
-      const T k = mu_g * (-v[1]) / (vt * vt * vt) * gdot;
-      gv[0] = r.scale * gout[0] + k * v[0];
-      gv[2] = r.scale * gout[2] + k * v[2];
-      gv[1] = mu_g * gdot / vt;
-      gmu += v[1] * gdot / vt;
+      // written with the unit tangent t and 1 - scale = mu |vn| / |vt|, both
+      // bounded, so that tiny tangential speeds cannot overflow
+      const T tx = v[0] / r.vt, tz = v[2] / r.vt;
+      const T gh = gout[0] * tx + gout[2] * tz;
+      const T one_m = T(1) - r.scale;
+      gv[0] = r.scale * gout[0] + one_m * gh * tx;
+      gv[2] = r.scale * gout[2] + one_m * gh * tz;
+      gv[1] = mu_g * gh;
+      gmu += v[1] * gh;
     } else {
       gv[0] = gv[2] = T(0);
     }

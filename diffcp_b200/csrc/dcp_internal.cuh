@@ -2,14 +2,18 @@
 // shared by the substep kernels.
 //
 // HBM layout (all instances concatenated, structure of arrays):
-//   state snapshot   [15][Nv] vertex  x(3) v(3) C(9)
-//                    [12][Nt] triangle C(9) d3(3)       (d cols 1-2 are edges)
-//                    [15][No] operator x v C
-//                    [15][Nc] cube     x v C
+//   state snapshot   [15][Nv] vertex  u(3) v(3) C(9)    u = x - x0 (displacement)
+//                    [12][Nt] triangle C(9) delta3(3)   delta3 = d3 - n0
+//                    [15][No] operator u v C
+//                    [15][Nc] cube     u v C
+//   rest             [9][Nt] D0^-1, [3][Nt] n0 (rest normal), [3][Nv], [3][No],
+//                    [3][Nc] rest positions x0
+// Positions and the triangle's third column are stored relative to the rest
+// configuration so that float32 keeps the small strains that drive the stress
+// (absolute positions near 0.5 would leave ~1e-5 strain resolution).
 //   grid             block-major per instance: 4x4x4-node blocks of 64 nodes,
 //                    float4 (p.xyz, m) / (v_out.xyz, 0) / adjoint per node
 //   topology         [3][Nt] global vertex ids, vertex->(corner, triangle) CSR
-//   rest shape       [9][Nt] D0^-1 (row-major entries)
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -87,6 +91,23 @@ __host__ __device__ inline StateP state_ptrs(float* base, int nv, int nt, int no
   s.o = s.t + 12LL * nt;
   s.c = s.o + 15LL * no;
   return s;
+}
+
+struct RestP {
+  const float* Di;  // [9][nt]
+  const float* n0;  // [3][nt]
+  const float* xv;  // [3][nv]
+  const float* xo;  // [3][no]
+  const float* xc;  // [3][nc]
+};
+__host__ __device__ inline RestP rest_ptrs(const float* rest, int nv, int nt, int no) {
+  RestP r;
+  r.Di = rest;
+  r.n0 = rest + 9LL * nt;
+  r.xv = rest + 12LL * nt;
+  r.xo = r.xv + 3LL * nv;
+  r.xc = r.xo + 3LL * no;
+  return r;
 }
 
 __device__ __forceinline__ long long node_index(const InstDev& I, int i, int j, int k) {

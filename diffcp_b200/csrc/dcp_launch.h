@@ -2,26 +2,82 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "dcp_internal.cuh"
 
 namespace dcp {
 
+enum KernelId {
+  KID_TRI_FORWARD = 0, KID_POINT_P2G, KID_GRID, KID_G2P, KID_G2P_ADJ, KID_GRID_ADJ, KID_POINT_ADJ, KID_TRI_ADJ,
+  KID_VERTEX_COLLECT, KID_CHAMFER_FWD, KID_CHAMFER_LOSS, KID_CHAMFER_BWD, KID_INIT, KID_COUNT
+};
+extern const char* const kKernelNames[KID_COUNT];
+
+// Launch accounting: counts every kernel issued and, when `timing` is on,
+// brackets each launch with a pair of CUDA events on its stream.
+struct Profiler {
+  bool timing = false;
+  long long launches = 0;
+  struct Rec {
+    int id;
+    cudaEvent_t a, b;
+  };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  cudaEvent_t take() {
+    if (pool.empty()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      return e;
+    }
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+  }
+};
+
+struct ProfScope {
+  Profiler* p;
+  cudaStream_t s;
+  int id;
+  cudaEvent_t a = nullptr;
+  ProfScope(Profiler* p_, int id_, cudaStream_t s_) : p(p_), s(s_), id(id_) {
+    if (p) {
+      ++p->launches;
+      if (p->timing) {
+        a = p->take();
+        cudaEventRecord(a, s);
+      }
+    }
+  }
+  ~ProfScope() {
+    if (p && p->timing) {
+      cudaEvent_t b = p->take();
+      cudaEventRecord(b, s);
+      p->recs.push_back(Profiler::Rec{id, a, b});
+    }
+  }
+};
+
 struct LaunchCfg {
   int block;      // threads per CTA = particles per chunk
   int grid_ctas;  // CTAs of the persistent grid-update kernels
+  Profiler* prof = nullptr;
 };
 
 cudaError_t configure_kernels(const BatchDev& B);
-cudaError_t launch_init(const BatchDev& B, const float* x0v, const float* x0o, const float* x0c, float* state, float* rest,
-                        cudaStream_t s);
+cudaError_t launch_init(const BatchDev& B, const LaunchCfg& L, const float* x0v, const float* x0o, const float* x0c,
+                        float* state, float* rest, cudaStream_t s);
 cudaError_t launch_forward(const BatchDev& B, const LaunchCfg& L, const float* params, const float* traj, const float* rest,
                            int step, int window, const float* sin, float* sout, cudaStream_t s);
 cudaError_t launch_backward(const BatchDev& B, const LaunchCfg& L, const float* params, const float* traj,
                             const float* rest, int step, int window, const float* sin, const float* aout, float* ain,
                             double* gparams, double* gtraj, cudaStream_t s);
-cudaError_t launch_chamfer_forward(const BatchDev& B, int max_nq, const float* state, const float* targets, int* qarg,
-                                   float* loss, cudaStream_t s);
-cudaError_t launch_chamfer_backward(const BatchDev& B, int max_nq, const float* state, const float* targets,
-                                    const int* qarg, const float* gloss, float* adj, cudaStream_t s);
+cudaError_t launch_chamfer_forward(const BatchDev& B, const LaunchCfg& L, int max_nq, const float* rest,
+                                   const float* state, const float* targets, int* qarg, float* loss, cudaStream_t s);
+cudaError_t launch_chamfer_backward(const BatchDev& B, const LaunchCfg& L, int max_nq, const float* rest,
+                                    const float* state, const float* targets, const int* qarg, const float* gloss,
+                                    float* adj, cudaStream_t s);
 
 }  // namespace dcp

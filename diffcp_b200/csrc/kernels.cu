@@ -30,24 +30,27 @@ __device__ __forceinline__ float3 ld3(const float* base, long long stride, long 
 }
 
 // ============================================================== init
-// initialize_ti_field (simulation.py:447-477): zero velocities and affine
-// matrices, triangle d = [e1, e2, n] with n the normalised cross product of the
-// eps-normalised edges (norm(1e-6)), rest-shape inverse D0^-1.
+// initialize_ti_field (simulation.py:447-477): zero displacements, velocities
+// and affine matrices; rest positions x0; triangle rest normal n0 = the
+// normalised cross product of the eps-normalised edges (norm(1e-6)) and the
+// rest-shape inverse D0^-1 of D0 = [e1, e2, n0].
 __global__ void k_init(BatchDev B, const float* __restrict__ x0v, const float* __restrict__ x0o,
                        const float* __restrict__ x0c, float* __restrict__ state, float* __restrict__ rest) {
   StateP S = state_ptrs(state, B.nv, B.nt, B.no);
+  RestP R = rest_ptrs(rest, B.nv, B.nt, B.no);
   const long long total = (long long)B.nv + B.no + B.nc + B.nt;
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
     long long i = g;
     if (i < B.nv + B.no + B.nc) {
       float* dst;
+      float* rdst;
       const float* src;
       long long n, p;
-      if (i < B.nv) { dst = S.v; src = x0v; n = B.nv; p = i; }
-      else if (i < B.nv + B.no) { dst = S.o; src = x0o; n = B.no; p = i - B.nv; }
-      else { dst = S.c; src = x0c; n = B.nc; p = i - B.nv - B.no; }
-      for (int c = 0; c < 3; ++c) dst[c * n + p] = src[c * n + p];
-      for (int c = 3; c < 15; ++c) dst[c * n + p] = 0.f;
+      if (i < B.nv) { dst = S.v; rdst = const_cast<float*>(R.xv); src = x0v; n = B.nv; p = i; }
+      else if (i < B.nv + B.no) { dst = S.o; rdst = const_cast<float*>(R.xo); src = x0o; n = B.no; p = i - B.nv; }
+      else { dst = S.c; rdst = const_cast<float*>(R.xc); src = x0c; n = B.nc; p = i - B.nv - B.no; }
+      for (int c = 0; c < 3; ++c) rdst[c * n + p] = src[c * n + p];
+      for (int c = 0; c < 15; ++c) dst[c * n + p] = 0.f;
       continue;
     }
     const long long t = i - (B.nv + B.no + B.nc);
@@ -71,34 +74,41 @@ __global__ void k_init(BatchDev B, const float* __restrict__ x0v, const float* _
     const float det = m00 * c00 + m01 * c10 + m02 * c20;
     const float id = 1.f / det;
     const float inv[9] = {c00 * id, c01 * id, c02 * id, c10 * id, c11 * id, c12 * id, c20 * id, c21 * id, c22 * id};
-    for (int q = 0; q < 9; ++q) {
-      rest[q * (long long)B.nt + t] = inv[q];
-      S.t[q * (long long)B.nt + t] = 0.f;
-    }
-    S.t[9 * (long long)B.nt + t] = nx;
-    S.t[10 * (long long)B.nt + t] = ny;
-    S.t[11 * (long long)B.nt + t] = nz;
+    float* Di = const_cast<float*>(R.Di);
+    float* n0 = const_cast<float*>(R.n0);
+    for (int q = 0; q < 9; ++q) Di[q * (long long)B.nt + t] = inv[q];
+    for (int q = 0; q < 12; ++q) S.t[q * (long long)B.nt + t] = 0.f;
+    n0[t] = nx;
+    n0[(long long)B.nt + t] = ny;
+    n0[2 * (long long)B.nt + t] = nz;
   }
 }
 
-// Triangle geometry at one state: vertex ids, positions, velocities, centroid.
+// Triangle geometry at one state: vertex ids, rest positions, displacements,
+// absolute positions, velocities, centroid.
 struct TriGeom {
   int vid[3];
-  float X[3][3];  // [corner][axis]
+  float X0[3][3];  // [corner][axis]
+  float U[3][3];
   float V[3][3];
   float xc[3], vc[3];
 };
-__device__ __forceinline__ void load_tri(const BatchDev& B, const StateP& S, long long t, bool need_v, TriGeom& g) {
+__device__ __forceinline__ void load_tri(const BatchDev& B, const StateP& S, const RestP& R, long long t, bool need_v,
+                                         TriGeom& g) {
   const long long nv = B.nv, nt = B.nt;
 #pragma unroll
   for (int c = 0; c < 3; ++c) g.vid[c] = __ldg(B.tri_v + c * nt + t);
 #pragma unroll
   for (int c = 0; c < 3; ++c)
 #pragma unroll
-    for (int a = 0; a < 3; ++a) g.X[c][a] = __ldg(S.v + a * nv + g.vid[c]);
+    for (int a = 0; a < 3; ++a) {
+      g.X0[c][a] = __ldg(R.xv + a * nv + g.vid[c]);
+      g.U[c][a] = __ldg(S.v + a * nv + g.vid[c]);
+    }
   const float third = 1.f / 3.f;
 #pragma unroll
-  for (int a = 0; a < 3; ++a) g.xc[a] = third * ((g.X[0][a] + g.X[1][a]) + g.X[2][a]);
+  for (int a = 0; a < 3; ++a)
+    g.xc[a] = third * (((g.X0[0][a] + g.U[0][a]) + (g.X0[1][a] + g.U[1][a])) + (g.X0[2][a] + g.U[2][a]));
   if (need_v) {
 #pragma unroll
     for (int c = 0; c < 3; ++c)
@@ -109,19 +119,38 @@ __device__ __forceinline__ void load_tri(const BatchDev& B, const StateP& S, lon
   }
 }
 
-// F = d D0^-1 with d = [x2 - x1, x3 - x1, d3] (simulation.py:395-407).
-__device__ __forceinline__ void tri_F(const TriGeom& g, const float d3[3], const float Di[9], M3<float>& d, M3<float>& F) {
+// d = [x2 - x1, x3 - x1, d3] and F = d D0^-1 (simulation.py:395-407), returned
+// as the deviation Fe = F - I = (d - D0) D0^-1 with d - D0 formed from
+// displacements and delta3 = d3 - n0.
+__device__ __forceinline__ void tri_F(const TriGeom& g, const float dl3[3], const float n0[3], const float Di[9],
+                                      M3<float>& d, M3<float>& Fe) {
+  float dd[9];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    d.m[3 * a + 0] = g.X[1][a] - g.X[0][a];
-    d.m[3 * a + 1] = g.X[2][a] - g.X[0][a];
-    d.m[3 * a + 2] = d3[a];
+    dd[3 * a + 0] = g.U[1][a] - g.U[0][a];
+    dd[3 * a + 1] = g.U[2][a] - g.U[0][a];
+    dd[3 * a + 2] = dl3[a];
+    d.m[3 * a + 0] = (g.X0[1][a] - g.X0[0][a]) + dd[3 * a + 0];
+    d.m[3 * a + 1] = (g.X0[2][a] - g.X0[0][a]) + dd[3 * a + 1];
+    d.m[3 * a + 2] = n0[a] + dl3[a];
   }
 #pragma unroll
   for (int r = 0; r < 3; ++r)
 #pragma unroll
     for (int c = 0; c < 3; ++c)
-      F.m[3 * r + c] = d.m[3 * r] * Di[c] + d.m[3 * r + 1] * Di[3 + c] + d.m[3 * r + 2] * Di[6 + c];
+      Fe.m[3 * r + c] = dd[3 * r] * Di[c] + dd[3 * r + 1] * Di[3 + c] + dd[3 * r + 2] * Di[6 + c];
+}
+
+__device__ __forceinline__ void load_tri_rest(const BatchDev& B, const RestP& R, const StateP& S, long long t,
+                                              float dl3[3], float n0[3], float Di[9]) {
+  const long long nt = B.nt;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    dl3[q] = __ldg(S.t + (9 + q) * nt + t);
+    n0[q] = __ldg(R.n0 + q * nt + t);
+  }
+#pragma unroll
+  for (int q = 0; q < 9; ++q) Di[q] = __ldg(R.Di + q * nt + t);
 }
 
 __device__ __forceinline__ void lame(float E, float nu, float& mu, float& la) {
@@ -140,10 +169,11 @@ __global__ void __launch_bounds__(256) k_tri_forward(BatchDev B, const float* __
   const long long t = ch.start + threadIdx.x;
   const long long nt = B.nt;
   StateP S = state_ptrs(const_cast<float*>(sin), B.nv, B.nt, B.no);
+  const RestP R = rest_ptrs(rest, B.nv, B.nt, B.no);
   TriGeom g;
   Sten st;
   if (valid) {
-    load_tri(B, S, t, true, g);
+    load_tri(B, S, R, t, true, g);
     make_stencil(g.xc, I, st, B.status, ch.inst);
   }
   tile_setup(T, st.base, valid, B.tile_nodes);
@@ -155,17 +185,15 @@ __global__ void __launch_bounds__(256) k_tri_forward(BatchDev B, const float* __
     float mu, la;
     lame(prm[PRM_E], prm[PRM_NU], mu, la);
     const float ks = prm[PRM_KS], kc = prm[PRM_KC];
-    float C[9], d3[3], Di[9];
+    float C[9], dl3[3], n0[3], Di[9];
 #pragma unroll
     for (int q = 0; q < 9; ++q) C[q] = __ldg(S.t + q * nt + t);
-#pragma unroll
-    for (int q = 0; q < 3; ++q) d3[q] = __ldg(S.t + (9 + q) * nt + t);
-#pragma unroll
-    for (int q = 0; q < 9; ++q) Di[q] = __ldg(rest + q * nt + t);
-    M3<float> d, F;
-    tri_F(g, d3, Di, d, F);
+    load_tri_rest(B, R, S, t, dl3, n0, Di);
+    M3<float> d, Fe;
+    tri_F(g, dl3, n0, Di, d, Fe);
+    const float d3[3] = {d.m[2], d.m[5], d.m[8]};
     Stress<float> sts;
-    stress_forward<float>(F, mu, la, ks, kc, sts);
+    stress_forward<float>(Fe, mu, la, ks, kc, sts);
     const M3<float>& P = sts.P;
     const float vol = I.vol_q, dt = B.dt, m = I.m_q, dx = I.dx, inv_dx = I.inv_dx;
     // per-corner in-plane forces with r1 = (D0^-1[0,0], d[0,1], d[0,2]),
@@ -216,6 +244,9 @@ __device__ __forceinline__ void point_arrays(const BatchDev& B, const StateP& S,
   else if (kind == CHUNK_OPERATOR) { base = S.o; n = B.no; }
   else { base = S.c; n = B.nc; }
 }
+__device__ __forceinline__ const float* point_rest(const RestP& R, int kind) {
+  return kind == CHUNK_VERTEX ? R.xv : (kind == CHUNK_OPERATOR ? R.xo : R.xc);
+}
 
 // Operator target velocity of simulation.py:160-165 (keyframe index in float32).
 __device__ __forceinline__ bool operator_velocity(const BatchDev& B, const InstDev& I, const float* traj, int step,
@@ -235,7 +266,7 @@ __device__ __forceinline__ bool operator_velocity(const BatchDev& B, const InstD
 }
 
 __global__ void __launch_bounds__(256) k_point_p2g(BatchDev B, const float* __restrict__ traj, int step, int window,
-                                                   const float* __restrict__ sin) {
+                                                   const float* __restrict__ rest, const float* __restrict__ sin) {
   extern __shared__ float4 tile[];
   __shared__ TileHdr T;
   const Chunk ch = B.chunks[B.n_tri_chunks + blockIdx.x];
@@ -246,11 +277,12 @@ __global__ void __launch_bounds__(256) k_point_p2g(BatchDev B, const float* __re
   float* arr;
   long long n;
   point_arrays(B, S, ch.kind, arr, n);
+  const float* x0 = point_rest(rest_ptrs(rest, B.nv, B.nt, B.no), ch.kind);
   float X[3];
   Sten st;
   if (valid) {
 #pragma unroll
-    for (int a = 0; a < 3; ++a) X[a] = __ldg(arr + a * n + p);
+    for (int a = 0; a < 3; ++a) X[a] = __ldg(x0 + a * n + p) + __ldg(arr + a * n + p);
     make_stencil(X, I, st, B.status, ch.inst);
   }
   tile_setup(T, st.base, valid, B.tile_nodes);
@@ -368,17 +400,19 @@ __device__ __forceinline__ float3 gv(const BatchDev& B, const InstDev& I, int i,
 }
 
 __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict__ params,
-                                             const float* __restrict__ sin, float* __restrict__ sout) {
+                                             const float* __restrict__ rest, const float* __restrict__ sin,
+                                             float* __restrict__ sout) {
   const Chunk ch = B.chunks[blockIdx.x];
   if (threadIdx.x >= ch.count) return;
   const InstDev& I = B.inst[ch.inst];
   StateP Si = state_ptrs(const_cast<float*>(sin), B.nv, B.nt, B.no);
   StateP So = state_ptrs(sout, B.nv, B.nt, B.no);
+  const RestP R = rest_ptrs(rest, B.nv, B.nt, B.no);
   const float dt = B.dt, inv_dx = I.inv_dx;
   if (ch.kind == CHUNK_TRI) {
     const long long t = ch.start + threadIdx.x, nt = B.nt;
     TriGeom g;
-    load_tri(B, Si, t, false, g);
+    load_tri(B, Si, R, t, false, g);
     Sten st;
     make_stencil(g.xc, I, st, B.status, ch.inst);
     float Ct[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -409,10 +443,13 @@ __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict
         const float sy = 0.5f * (Ct[3 * a + b] + Ct[3 * b + a]);
         Cn[3 * a + b] = sk + keep * sy;
       }
-    float d3[3];
+    float dl3[3], d3[3];
 #pragma unroll
-    for (int q = 0; q < 3; ++q) d3[q] = __ldg(Si.t + (9 + q) * nt + t);
-    // d3 += (dt C + dt^2/2 C C) d3 (simulation.py:397-400)
+    for (int q = 0; q < 3; ++q) {
+      dl3[q] = __ldg(Si.t + (9 + q) * nt + t);
+      d3[q] = __ldg(R.n0 + q * nt + t) + dl3[q];
+    }
+    // d3 += (dt C + dt^2/2 C C) d3 (simulation.py:397-400), kept as delta3 = d3 - n0
     float Md[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -429,17 +466,21 @@ __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict
 #pragma unroll
     for (int q = 0; q < 9; ++q) So.t[q * nt + t] = Cn[q];
 #pragma unroll
-    for (int q = 0; q < 3; ++q) So.t[(9 + q) * nt + t] = d3[q] + Md[q];
+    for (int q = 0; q < 3; ++q) So.t[(9 + q) * nt + t] = dl3[q] + Md[q];
     return;
   }
   float *ai, *ao;
   long long n;
   point_arrays(B, Si, ch.kind, ai, n);
   point_arrays(B, So, ch.kind, ao, n);
+  const float* x0 = point_rest(R, ch.kind);
   const long long p = ch.start + threadIdx.x;
-  float X[3];
+  float X[3], U[3];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) X[a] = __ldg(ai + a * n + p);
+  for (int a = 0; a < 3; ++a) {
+    U[a] = __ldg(ai + a * n + p);
+    X[a] = __ldg(x0 + a * n + p) + U[a];
+  }
   Sten st;
   make_stencil(X, I, st, B.status, ch.inst);
   float v[3] = {0.f, 0.f, 0.f}, C[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -464,7 +505,7 @@ __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict
   bool finite = true;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    ao[a * n + p] = X[a] + dt * v[a];
+    ao[a * n + p] = U[a] + dt * v[a];
     ao[(3 + a) * n + p] = v[a];
     finite = finite && isfinite(v[a]);
   }
@@ -478,8 +519,9 @@ __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict
 // the position adjoint of the gather; triangle: reverse of the d3 update and of
 // the skew/sym damping.
 __global__ void __launch_bounds__(256) k_g2p_adj(BatchDev B, const float* __restrict__ params,
-                                                 const float* __restrict__ sin, const float* __restrict__ aout,
-                                                 float* __restrict__ ain, double* __restrict__ gparams) {
+                                                 const float* __restrict__ rest, const float* __restrict__ sin,
+                                                 const float* __restrict__ aout, float* __restrict__ ain,
+                                                 double* __restrict__ gparams) {
   extern __shared__ float4 tile[];
   __shared__ TileHdr T;
   const Chunk ch = B.chunks[blockIdx.x];
@@ -488,6 +530,7 @@ __global__ void __launch_bounds__(256) k_g2p_adj(BatchDev B, const float* __rest
   StateP Si = state_ptrs(const_cast<float*>(sin), B.nv, B.nt, B.no);
   StateP Ao = state_ptrs(const_cast<float*>(aout), B.nv, B.nt, B.no);
   StateP Ai = state_ptrs(ain, B.nv, B.nt, B.no);
+  const RestP R = rest_ptrs(rest, B.nv, B.nt, B.no);
   const float dt = B.dt, inv_dx = I.inv_dx;
   const bool tri = ch.kind == CHUNK_TRI;
   const long long idx = ch.start + threadIdx.x;
@@ -503,11 +546,12 @@ __global__ void __launch_bounds__(256) k_g2p_adj(BatchDev B, const float* __rest
   }
   if (valid) {
     if (tri) {
-      load_tri(B, Si, idx, false, g);
+      load_tri(B, Si, R, idx, false, g);
       X[0] = g.xc[0]; X[1] = g.xc[1]; X[2] = g.xc[2];
     } else {
+      const float* x0 = point_rest(R, ch.kind);
 #pragma unroll
-      for (int a = 0; a < 3; ++a) X[a] = __ldg(ai + a * n + idx);
+      for (int a = 0; a < 3; ++a) X[a] = __ldg(x0 + a * n + idx) + __ldg(ai + a * n + idx);
     }
     make_stencil(X, I, st, B.status, ch.inst);
   }
@@ -551,7 +595,7 @@ __global__ void __launch_bounds__(256) k_g2p_adj(BatchDev B, const float* __rest
       float d3[3], bd3o[3], bCo[9];
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
-        d3[q] = __ldg(Si.t + (9 + q) * nt + idx);
+        d3[q] = __ldg(R.n0 + q * nt + idx) + __ldg(Si.t + (9 + q) * nt + idx);
         bd3o[q] = __ldg(Ao.t + (9 + q) * nt + idx);
       }
 #pragma unroll
@@ -699,8 +743,8 @@ __device__ __forceinline__ float4 gadj(const BatchDev& B, const InstDev& I, int 
 
 // Reverse of k_point_p2g: gather dL/dp, dL/dm over the stencil.
 __global__ void __launch_bounds__(256) k_point_adj(BatchDev B, const float* __restrict__ traj, int step, int window,
-                                                   const float* __restrict__ sin, float* __restrict__ ain,
-                                                   double* __restrict__ gtraj) {
+                                                   const float* __restrict__ rest, const float* __restrict__ sin,
+                                                   float* __restrict__ ain, double* __restrict__ gtraj) {
   const Chunk ch = B.chunks[B.n_tri_chunks + blockIdx.x];
   if (threadIdx.x >= ch.count) return;
   const InstDev& I = B.inst[ch.inst];
@@ -710,10 +754,11 @@ __global__ void __launch_bounds__(256) k_point_adj(BatchDev B, const float* __re
   long long n;
   point_arrays(B, Si, ch.kind, ai, n);
   point_arrays(B, Ai, ch.kind, aa, n);
+  const float* x0 = point_rest(rest_ptrs(rest, B.nv, B.nt, B.no), ch.kind);
   const long long p = ch.start + threadIdx.x;
   float X[3];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) X[a] = __ldg(ai + a * n + p);
+  for (int a = 0; a < 3; ++a) X[a] = __ldg(x0 + a * n + p) + __ldg(ai + a * n + p);
   Sten st;
   make_stencil(X, I, st, B.status, ch.inst);
   float m, base_v[3] = {0.f, 0.f, 0.f};
@@ -811,6 +856,7 @@ __global__ void __launch_bounds__(128) k_tri_adj(BatchDev B, const float* __rest
   const long long t = ch.start + threadIdx.x, nt = B.nt;
   StateP Si = state_ptrs(const_cast<float*>(sin), B.nv, B.nt, B.no);
   StateP Ai = state_ptrs(ain, B.nv, B.nt, B.no);
+  const RestP R = rest_ptrs(rest, B.nv, B.nt, B.no);
   const float* prm = params + ch.inst * PRM_STRIDE;
   float E = prm[PRM_E], nu = prm[PRM_NU];
   float mu, la;
@@ -819,20 +865,18 @@ __global__ void __launch_bounds__(128) k_tri_adj(BatchDev B, const float* __rest
   float gsum[4] = {0.f, 0.f, 0.f, 0.f};
   if (valid) {
     TriGeom g;
-    load_tri(B, Si, t, true, g);
+    load_tri(B, Si, R, t, true, g);
     Sten st;
     make_stencil(g.xc, I, st, B.status, ch.inst);
-    float C[9], d3[3], Di[9];
+    float C[9], dl3[3], n0[3], Di[9];
 #pragma unroll
     for (int q = 0; q < 9; ++q) C[q] = __ldg(Si.t + q * nt + t);
-#pragma unroll
-    for (int q = 0; q < 3; ++q) d3[q] = __ldg(Si.t + (9 + q) * nt + t);
-#pragma unroll
-    for (int q = 0; q < 9; ++q) Di[q] = __ldg(rest + q * nt + t);
-    M3<float> d, F;
-    tri_F(g, d3, Di, d, F);
+    load_tri_rest(B, R, Si, t, dl3, n0, Di);
+    M3<float> d, Fe;
+    tri_F(g, dl3, n0, Di, d, Fe);
+    const float d3[3] = {d.m[2], d.m[5], d.m[8]};
     Stress<float> sts;
-    stress_forward<float>(F, mu, la, ks, kc, sts);
+    stress_forward<float>(Fe, mu, la, ks, kc, sts);
     const float vol = I.vol_q, dt = B.dt, m = I.m_q, dx = I.dx, inv_dx = I.inv_dx;
     const float cn = -vol * dt;
     const float P3[3] = {sts.P.m[2], sts.P.m[5], sts.P.m[8]};
@@ -973,10 +1017,12 @@ __global__ void k_vertex_collect(BatchDev B, float* __restrict__ ain) {
 // compute_loss (parameter_fitting_functions.py:3-15): for every target point
 // the minimum over vertices of |x - t|^2 / 3, evaluated with the reference's
 // float32 operation order; ties go to the vertex of lowest rank.
-__global__ void __launch_bounds__(128) k_chamfer_fwd(BatchDev B, const float* __restrict__ state,
-                                                     const float* __restrict__ targets, int* __restrict__ qarg) {
-  __shared__ float sx[256], sy[256], sz[256];
+__global__ void __launch_bounds__(128) k_chamfer_fwd(BatchDev B, const float* __restrict__ rest,
+                                                     const float* __restrict__ state, const float* __restrict__ targets,
+                                                     int* __restrict__ qarg) {
+  __shared__ float sx[256], sy[256], sz[256], ux[256], uy[256], uz[256];
   __shared__ int sr[256];
+  const RestP R = rest_ptrs(rest, B.nv, B.nt, B.no);
   const int inst = blockIdx.y;
   const InstDev& I = B.inst[inst];
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -997,9 +1043,12 @@ __global__ void __launch_bounds__(128) k_chamfer_fwd(BatchDev B, const float* __
       const int v = base + j;
       if (v < I.nv) {
         const long long gv = I.v_off + v;
-        sx[j] = __ldg(state + gv);
-        sy[j] = __ldg(state + nv + gv);
-        sz[j] = __ldg(state + 2 * nv + gv);
+        sx[j] = __ldg(R.xv + gv);
+        sy[j] = __ldg(R.xv + nv + gv);
+        sz[j] = __ldg(R.xv + 2 * nv + gv);
+        ux[j] = __ldg(state + gv);
+        uy[j] = __ldg(state + nv + gv);
+        uz[j] = __ldg(state + 2 * nv + gv);
         sr[j] = __ldg(B.vertex_rank + gv);
       }
     }
@@ -1007,7 +1056,10 @@ __global__ void __launch_bounds__(128) k_chamfer_fwd(BatchDev B, const float* __
     const int cnt = min(256, I.nv - base);
     if (valid) {
       for (int j = 0; j < cnt; ++j) {
-        const float dx = __fsub_rn(sx[j], tx), dy = __fsub_rn(sy[j], ty), dz = __fsub_rn(sz[j], tz);
+        // x - t = (x0 - t) + u
+        const float dx = __fadd_rn(__fsub_rn(sx[j], tx), ux[j]);
+        const float dy = __fadd_rn(__fsub_rn(sy[j], ty), uy[j]);
+        const float dz = __fadd_rn(__fsub_rn(sz[j], tz), uz[j]);
         const float dd = __fdiv_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)), 3.f);
         if (dd < best || (dd == best && sr[j] < brank)) {
           best = dd;
@@ -1040,8 +1092,10 @@ __global__ void k_chamfer_loss(BatchDev B, float* __restrict__ loss) {
   }
 }
 
-__global__ void k_chamfer_bwd(BatchDev B, const float* __restrict__ state, const float* __restrict__ targets,
-                              const int* __restrict__ qarg, const float* __restrict__ gloss, float* __restrict__ adj) {
+__global__ void k_chamfer_bwd(BatchDev B, const float* __restrict__ rest, const float* __restrict__ state,
+                              const float* __restrict__ targets, const int* __restrict__ qarg,
+                              const float* __restrict__ gloss, float* __restrict__ adj) {
+  const RestP R = rest_ptrs(rest, B.nv, B.nt, B.no);
   const int inst = blockIdx.y;
   const InstDev& I = B.inst[inst];
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1053,19 +1107,28 @@ __global__ void k_chamfer_bwd(BatchDev B, const float* __restrict__ state, const
   const float s = __ldg(gloss + inst) / (float)I.nq * (2.f / 3.f);
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const float d = __ldg(state + a * nv + v) - __ldg(targets + a * nq + gq);
+    const float d = (__ldg(R.xv + a * nv + v) - __ldg(targets + a * nq + gq)) + __ldg(state + a * nv + v);
     atomicAdd(adj + a * nv + v, s * d);
   }
 }
 
 // ============================================================== launchers
-static inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+const char* const kKernelNames[KID_COUNT] = {
+    "k_tri_forward", "k_point_p2g", "k_grid", "k_g2p", "k_g2p_adj", "k_grid_adj", "k_point_adj", "k_tri_adj",
+    "k_vertex_collect", "k_chamfer_fwd", "k_chamfer_loss", "k_chamfer_bwd", "k_init"};
 
-cudaError_t launch_init(const BatchDev& B, const float* x0v, const float* x0o, const float* x0c, float* state, float* rest,
-                        cudaStream_t s) {
+static inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+#define DCP_LAUNCH(id, ...)                   \
+  do {                                        \
+    ProfScope _scope(L.prof, (id), s);        \
+    __VA_ARGS__;                              \
+  } while (0)
+
+cudaError_t launch_init(const BatchDev& B, const LaunchCfg& L, const float* x0v, const float* x0o, const float* x0c,
+                        float* state, float* rest, cudaStream_t s) {
   const long long total = (long long)B.nv + B.no + B.nc + B.nt;
   const int grid = total > 0 ? (ceil_div(total, 256) < 148 * 16 ? ceil_div(total, 256) : 148 * 16) : 1;
-  k_init<<<grid, 256, 0, s>>>(B, x0v, x0o, x0c, state, rest);
+  DCP_LAUNCH(KID_INIT, (k_init<<<grid, 256, 0, s>>>(B, x0v, x0o, x0c, state, rest)));
   return cudaGetLastError();
 }
 
@@ -1074,10 +1137,13 @@ static inline size_t tile_bytes(const BatchDev& B) { return (size_t)B.tile_nodes
 cudaError_t launch_forward(const BatchDev& B, const LaunchCfg& L, const float* params, const float* traj, const float* rest,
                            int step, int window, const float* sin, float* sout, cudaStream_t s) {
   cudaMemsetAsync(B.counters, 0, sizeof(int), s);
-  if (B.n_tri_chunks) k_tri_forward<<<B.n_tri_chunks, L.block, tile_bytes(B), s>>>(B, params, rest, sin);
-  if (B.n_point_chunks) k_point_p2g<<<B.n_point_chunks, L.block, tile_bytes(B), s>>>(B, traj, step, window, sin);
-  k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_FORWARD);
-  k_g2p<<<B.n_tri_chunks + B.n_point_chunks, L.block, 0, s>>>(B, params, sin, sout);
+  if (B.n_tri_chunks)
+    DCP_LAUNCH(KID_TRI_FORWARD, (k_tri_forward<<<B.n_tri_chunks, L.block, tile_bytes(B), s>>>(B, params, rest, sin)));
+  if (B.n_point_chunks)
+    DCP_LAUNCH(KID_POINT_P2G,
+               (k_point_p2g<<<B.n_point_chunks, L.block, tile_bytes(B), s>>>(B, traj, step, window, rest, sin)));
+  DCP_LAUNCH(KID_GRID, (k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_FORWARD)));
+  DCP_LAUNCH(KID_G2P, (k_g2p<<<B.n_tri_chunks + B.n_point_chunks, L.block, 0, s>>>(B, params, rest, sin, sout)));
   return cudaGetLastError();
 }
 
@@ -1085,32 +1151,40 @@ cudaError_t launch_backward(const BatchDev& B, const LaunchCfg& L, const float* 
                             const float* rest, int step, int window, const float* sin, const float* aout, float* ain,
                             double* gparams, double* gtraj, cudaStream_t s) {
   cudaMemsetAsync(B.counters, 0, sizeof(int), s);
-  if (B.n_tri_chunks) k_tri_forward<<<B.n_tri_chunks, L.block, tile_bytes(B), s>>>(B, params, rest, sin);
-  if (B.n_point_chunks) k_point_p2g<<<B.n_point_chunks, L.block, tile_bytes(B), s>>>(B, traj, step, window, sin);
-  k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_RECOMPUTE);
-  k_g2p_adj<<<B.n_tri_chunks + B.n_point_chunks, L.block, tile_bytes(B), s>>>(B, params, sin, aout, ain, gparams);
-  k_grid_adj<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, gparams, gtraj);
-  if (B.n_point_chunks) k_point_adj<<<B.n_point_chunks, L.block, 0, s>>>(B, traj, step, window, sin, ain, gtraj);
-  if (B.n_tri_chunks) k_tri_adj<<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin, ain, gparams);
-  if (B.nv) k_vertex_collect<<<ceil_div(B.nv, 256), 256, 0, s>>>(B, ain);
+  if (B.n_tri_chunks)
+    DCP_LAUNCH(KID_TRI_FORWARD, (k_tri_forward<<<B.n_tri_chunks, L.block, tile_bytes(B), s>>>(B, params, rest, sin)));
+  if (B.n_point_chunks)
+    DCP_LAUNCH(KID_POINT_P2G,
+               (k_point_p2g<<<B.n_point_chunks, L.block, tile_bytes(B), s>>>(B, traj, step, window, rest, sin)));
+  DCP_LAUNCH(KID_GRID, (k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_RECOMPUTE)));
+  DCP_LAUNCH(KID_G2P_ADJ, (k_g2p_adj<<<B.n_tri_chunks + B.n_point_chunks, L.block, tile_bytes(B), s>>>(
+                              B, params, rest, sin, aout, ain, gparams)));
+  DCP_LAUNCH(KID_GRID_ADJ, (k_grid_adj<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, gparams, gtraj)));
+  if (B.n_point_chunks)
+    DCP_LAUNCH(KID_POINT_ADJ,
+               (k_point_adj<<<B.n_point_chunks, L.block, 0, s>>>(B, traj, step, window, rest, sin, ain, gtraj)));
+  if (B.n_tri_chunks)
+    DCP_LAUNCH(KID_TRI_ADJ, (k_tri_adj<<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin, ain, gparams)));
+  if (B.nv) DCP_LAUNCH(KID_VERTEX_COLLECT, (k_vertex_collect<<<ceil_div(B.nv, 256), 256, 0, s>>>(B, ain)));
   return cudaGetLastError();
 }
 
-cudaError_t launch_chamfer_forward(const BatchDev& B, int max_nq, const float* state, const float* targets, int* qarg,
-                                   float* loss, cudaStream_t s) {
+cudaError_t launch_chamfer_forward(const BatchDev& B, const LaunchCfg& L, int max_nq, const float* rest,
+                                   const float* state, const float* targets, int* qarg, float* loss, cudaStream_t s) {
   if (max_nq > 0) {
     dim3 grid(ceil_div(max_nq, 128), B.n_inst);
-    k_chamfer_fwd<<<grid, 128, 0, s>>>(B, state, targets, qarg);
+    DCP_LAUNCH(KID_CHAMFER_FWD, (k_chamfer_fwd<<<grid, 128, 0, s>>>(B, rest, state, targets, qarg)));
   }
-  k_chamfer_loss<<<B.n_inst, 256, 0, s>>>(B, loss);
+  DCP_LAUNCH(KID_CHAMFER_LOSS, (k_chamfer_loss<<<B.n_inst, 256, 0, s>>>(B, loss)));
   return cudaGetLastError();
 }
 
-cudaError_t launch_chamfer_backward(const BatchDev& B, int max_nq, const float* state, const float* targets,
-                                    const int* qarg, const float* gloss, float* adj, cudaStream_t s) {
+cudaError_t launch_chamfer_backward(const BatchDev& B, const LaunchCfg& L, int max_nq, const float* rest,
+                                    const float* state, const float* targets, const int* qarg, const float* gloss,
+                                    float* adj, cudaStream_t s) {
   if (max_nq > 0) {
     dim3 grid(ceil_div(max_nq, 128), B.n_inst);
-    k_chamfer_bwd<<<grid, 128, 0, s>>>(B, state, targets, qarg, gloss, adj);
+    DCP_LAUNCH(KID_CHAMFER_BWD, (k_chamfer_bwd<<<grid, 128, 0, s>>>(B, rest, state, targets, qarg, gloss, adj)));
   }
   return cudaGetLastError();
 }

@@ -25,6 +25,7 @@ EXPORTED = (
     "dcp_plan", "dcp_create", "dcp_destroy", "dcp_sizes", "dcp_init_state", "dcp_substep_forward",
     "dcp_substep_backward", "dcp_chamfer_forward", "dcp_chamfer_backward", "dcp_rollout_floats",
     "dcp_rollout_state_offset", "dcp_rollout_forward", "dcp_rollout_backward", "dcp_read_status", "dcp_last_error",
+    "dcp_launch_count", "dcp_profile", "dcp_profile_read", "dcp_kernel_count", "dcp_kernel_name",
 )
 
 
@@ -83,8 +84,8 @@ def lib():
                                       c_void_p]
     L.dcp_substep_backward.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_void_p,
                                        c_void_p, c_void_p, c_void_p, c_void_p]
-    L.dcp_chamfer_forward.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
-    L.dcp_chamfer_backward.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
+    L.dcp_chamfer_forward.argtypes = [c_void_p] * 7
+    L.dcp_chamfer_backward.argtypes = [c_void_p] * 8
     L.dcp_rollout_floats.argtypes = [c_void_p, c_int32, c_int32]
     L.dcp_rollout_floats.restype = c_int64
     L.dcp_rollout_state_offset.argtypes = [c_void_p, c_int32, c_int32, c_int32]
@@ -95,6 +96,13 @@ def lib():
                                        c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p]
     L.dcp_read_status.argtypes = [c_void_p, P(c_int32), c_int32, c_void_p]
     L.dcp_last_error.restype = ctypes.c_char_p
+    L.dcp_launch_count.argtypes = [c_void_p]
+    L.dcp_launch_count.restype = c_int64
+    L.dcp_profile.argtypes = [c_void_p, c_int32]
+    L.dcp_profile_read.argtypes = [c_void_p, P(ctypes.c_double), P(c_int64)]
+    L.dcp_kernel_count.restype = c_int32
+    L.dcp_kernel_name.argtypes = [c_int32]
+    L.dcp_kernel_name.restype = ctypes.c_char_p
     for name in EXPORTED:
         getattr(L, name)
     _LIB = L

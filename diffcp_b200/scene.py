@@ -187,12 +187,13 @@ def regular_sheet(n: int, side: float):
 
 
 def cubic_spline_grasp(start: np.ndarray, n_steps: int, dt: float, rng: np.random.Generator, n_ctrl: int = 5,
-                       amplitude: float = 0.05):
-    """Smooth gripper path through ``n_ctrl`` control points: the first is the
-    grasped corner, the others are offset by U(-amplitude, amplitude) per axis.
-    Returns per-substep velocities and centres, each (n_steps, 3)."""
+                       amplitude: float = 0.05, duration: float = 1.0):
+    """Smooth gripper path through ``n_ctrl`` control points spread over
+    ``duration`` seconds: the first is the grasped corner, the others are
+    offset by U(-amplitude, amplitude) per axis.  Returns per-substep
+    velocities and centres, each (n_steps, 3)."""
     from scipy.interpolate import CubicSpline
-    T = n_steps * dt
+    T = max(duration, n_steps * dt)
     tk = np.linspace(0.0, T, n_ctrl)
     pts = start[None, :] + np.concatenate([np.zeros((1, 3)), rng.uniform(-amplitude, amplitude, (n_ctrl - 1, 3))])
     cs = CubicSpline(tk, pts, axis=0, bc_type="clamped")
@@ -203,7 +204,8 @@ def cubic_spline_grasp(start: np.ndarray, n_steps: int, dt: float, rng: np.rando
 def sheet_scene(n: int = 32, side: float = 0.2, height: float = 0.3, n_grid: int = 64, dt: float = 2e-4,
                 n_steps: int = 200, E: float = 5e3, nu: float = 0.3, density: float = 0.2, friction: float = 0.3,
                 damping: float = REFERENCE_DAMPING, seed: int = 0, n_targets: int = 2048,
-                gripper_radius: Optional[float] = None, center=(0.5, 0.5), velocities=None) -> ClothScene:
+                gripper_radius: Optional[float] = None, center=(0.5, 0.5), velocities=None,
+                spline_duration: float = 1.0) -> ClothScene:
     """Square cloth sheet held by two kinematic spheres at two adjacent
     corners, the cloth of the benchmark configurations.  Masses follow the
     reference's formulas (initialization.py:118-130) with the garment mass set
@@ -221,7 +223,7 @@ def sheet_scene(n: int = 32, side: float = 0.2, height: float = 0.3, n_grid: int
         vel = np.zeros((n_steps, 2, 3))
         cen = np.zeros((n_steps, 2, 3))
         for k in range(2):
-            vel[:, k], cen[:, k] = cubic_spline_grasp(corners[k], n_steps, dt, rng)
+            vel[:, k], cen[:, k] = cubic_spline_grasp(corners[k], n_steps, dt, rng, duration=spline_duration)
     else:
         vel = np.asarray(velocities, dtype=np.float64).reshape(n_steps, 2, 3)
         cen = corners[None] + dt * np.concatenate([np.zeros((1, 2, 3)), np.cumsum(vel, 0)[:-1]], 0)

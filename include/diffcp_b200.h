@@ -20,12 +20,16 @@
  *     component c of item i at c*N + i.  Particle and target arrays concatenate
  *     all instances in instance order.
  *
- * State snapshot (floats, dcp_plan().state_floats):
- *   [15][Nv] vertices  x(3) v(3) C(9, row-major)
- *   [12][Nt] triangles C(9) d3(3)   (d3 = advected third column of d;
- *                                    columns 1-2 of d are the current edges)
- *   [15][No] operator particles x v C
- *   [15][Nc] cube particles     x v C
+ * State snapshot (floats, dcp_plan().state_floats), relative to the rest
+ * configuration so that float32 resolves small strains:
+ *   [15][Nv] vertices  u(3) v(3) C(9, row-major)   u = x - x0
+ *   [12][Nt] triangles C(9) delta3(3)   delta3 = d3 - n0, d3 the advected third
+ *                                       column of d (columns 1-2 of d are the
+ *                                       current edges)
+ *   [15][No] operator particles u v C
+ *   [15][Nc] cube particles     u v C
+ * Rest buffer (floats, dcp_plan().rest_floats), written by dcp_init_state:
+ *   [9][Nt] D0^-1, [3][Nt] n0, [3][Nv] x0, [3][No] x0, [3][Nc] x0
  * Parameter table: [n_inst][8] floats: E, nu, shearing_stiffness,
  *   contact_stiffness, ground friction, damping, 0, 0.
  * Parameter gradients: [n_inst][8] doubles in the same order (accumulated).
@@ -91,7 +95,7 @@ typedef struct DcpOptions {
 typedef struct DcpSizes {
   int64_t n_vertex, n_tri, n_operator, n_cube, n_target; /* totals over the batch */
   int64_t state_floats;   /* one state snapshot */
-  int64_t rest_floats;    /* rest-shape inverses D0^-1, [9][Nt] */
+  int64_t rest_floats;    /* rest configuration: D0^-1, n0, x0 */
   int64_t traj_floats;    /* trajectory table */
   int64_t param_floats;   /* parameter table, 8 per instance */
   int64_t static_bytes;   /* device bytes for topology and launch tables */
@@ -115,8 +119,8 @@ int dcp_create(const DcpInstance* inst, int32_t n_inst, const DcpOptions* opt, c
 int dcp_destroy(DcpBatch* batch);
 int dcp_sizes(const DcpBatch* batch, DcpSizes* out);
 
-/* initialize_ti_field (simulation.py:447-477): state0 from rest positions
- * x0_* ([3][N] each) and the rest-shape inverses. */
+/* initialize_ti_field (simulation.py:447-477): rest buffer from the rest
+ * positions x0_* ([3][N] each) and the zero state0. */
 int dcp_init_state(DcpBatch* batch, const float* x0_vertex, const float* x0_operator, const float* x0_cube,
                    float* state0, float* rest, void* stream);
 
@@ -136,11 +140,11 @@ int dcp_substep_backward(DcpBatch* batch, const float* params, const float* traj
 /* compute_loss (parameter_fitting_functions.py:3-15) per instance: one-sided
  * Chamfer sum_q min_p |x_p - t_q|^2 / 3 / Nq on the vertices of `state`.
  * targets: [3][Nq_total]; argmin: [Nq_total] (global vertex index); loss: [n_inst]. */
-int dcp_chamfer_forward(DcpBatch* batch, const float* state, const float* targets, int32_t* argmin, float* loss,
-                        void* stream);
+int dcp_chamfer_forward(DcpBatch* batch, const float* rest, const float* state, const float* targets,
+                        int32_t* argmin, float* loss, void* stream);
 /* compute_loss.grad: adds dL/dx of the vertices into adj_state. */
-int dcp_chamfer_backward(DcpBatch* batch, const float* state, const float* targets, const int32_t* argmin,
-                         const float* grad_loss, float* adj_state, void* stream);
+int dcp_chamfer_backward(DcpBatch* batch, const float* rest, const float* state, const float* targets,
+                         const int32_t* argmin, const float* grad_loss, float* adj_state, void* stream);
 
 /* Rollout buffer of dcp_rollout_*: checkpoints every `ckpt_every` substeps plus
  * one recompute segment (floats). */
@@ -162,6 +166,19 @@ int dcp_rollout_forward(DcpBatch* batch, const float* params, const float* traj,
 int dcp_rollout_backward(DcpBatch* batch, const float* params, const float* traj, const float* rest, int32_t window,
                          int32_t n_steps, int32_t loss_step, int32_t ckpt_every, float* buf, float* adj_work,
                          double* grad_params, double* grad_traj, int32_t use_graph, void* stream);
+
+/* Kernel launch accounting.  dcp_launch_count: kernels issued on this batch
+ * so far (graph replays add the kernels of the captured graph).
+ * dcp_profile(1) brackets every subsequent launch with CUDA events on its
+ * stream (rollouts then run eagerly); dcp_profile_read fills per-kernel total
+ * milliseconds and launch counts, arrays of dcp_kernel_count() entries indexed
+ * like dcp_kernel_name(id).  Diagnostics only; no reference counterpart
+ * (the reference enables Taichi's kernel profiler, initialization.py:19-20). */
+int64_t dcp_launch_count(const DcpBatch* batch);
+int dcp_profile(DcpBatch* batch, int32_t enable);
+int dcp_profile_read(DcpBatch* batch, double* total_ms, int64_t* launches);
+int32_t dcp_kernel_count(void);
+const char* dcp_kernel_name(int32_t id);
 
 /* Per-instance DCP_STATUS_* bits (host array of n_inst); synchronises `stream`. */
 int dcp_read_status(DcpBatch* batch, int32_t* host_status, int32_t clear, void* stream);

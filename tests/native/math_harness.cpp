@@ -5,10 +5,17 @@
 
 using namespace dcp;
 
+// The kernels pass F - I; form it in double so the float build sees the exact deviation.
+template <class T>
+static M3<T> deviation(const double* F) {
+  M3<T> e;
+  for (int i = 0; i < 9; ++i) e.m[i] = T(F[i] - ((i % 4 == 0) ? 1.0 : 0.0));
+  return e;
+}
+
 template <class T>
 static void stress_fwd_T(const double* F, const double* prm, double* P) {
-  M3<T> f;
-  for (int i = 0; i < 9; ++i) f.m[i] = T(F[i]);
+  M3<T> f = deviation<T>(F);
   Stress<T> st;
   stress_forward<T>(f, T(prm[0]), T(prm[1]), T(prm[2]), T(prm[3]), st);
   for (int i = 0; i < 9; ++i) P[i] = double(st.P.m[i]);
@@ -16,11 +23,8 @@ static void stress_fwd_T(const double* F, const double* prm, double* P) {
 
 template <class T>
 static void stress_bwd_T(const double* F, const double* prm, const double* gP, int mode, double* gF, double* gprm) {
-  M3<T> f, gp, gf;
-  for (int i = 0; i < 9; ++i) {
-    f.m[i] = T(F[i]);
-    gp.m[i] = T(gP[i]);
-  }
+  M3<T> f = deviation<T>(F), gp, gf;
+  for (int i = 0; i < 9; ++i) gp.m[i] = T(gP[i]);
   Stress<T> st;
   stress_forward<T>(f, T(prm[0]), T(prm[1]), T(prm[2]), T(prm[3]), st);
   T gmu = 0, gla = 0, gks = 0, gkc = 0;

@@ -26,7 +26,7 @@ def _batch(scenes, **kw):
 
 def unpack(b, state, i=0):
     """Fields of instance i in the scene's original particle order (numpy)."""
-    f = b.state_fields(state)
+    f = b.absolute_fields(state)
     vp, tp = b.vperm[i], b.tperm[i]
     va, vb = int(b.v_off[i]), int(b.v_off[i + 1])
     ta, tb = int(b.t_off[i]), int(b.t_off[i + 1])
@@ -249,7 +249,7 @@ def test_chamfer_forward_argmin_and_backward():
         from oracle.sim64 import compute_loss
         lo, _ = compute_loss(x, torch.tensor(sc.targets, dtype=torch.float64))
         lo.backward()
-        got = b.vertex_x(adj, i).cpu().numpy()
+        got = b.vertex_x(adj, i, absolute=False).cpu().numpy()
         np.testing.assert_allclose(got, x.grad.numpy(), rtol=1e-4, atol=1e-4 * np.abs(x.grad.numpy()).max())
 
 

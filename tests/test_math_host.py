@@ -128,6 +128,9 @@ def test_grid_bc_forward_and_adjoint(lib, mu):
     ijk = rng.integers(0, G, size=(n, 3)).astype(np.int32)
     ijk[: n // 2, 1] = rng.integers(0, bound, size=n // 2)   # many floor nodes
     v = rng.standard_normal((n, 3))
+    v[:20, [0, 2]] *= 1e-22          # floor nodes with a denormal tangential speed
+    v[:20, 1] = -np.abs(v[:20, 1])
+    ijk[:20, 1] = 0
     out = np.zeros((n, 3))
     lib.h_grid_bc(n, _p(v), ijk.ctypes.data_as(_int), G, bound, ctypes.c_double(mu), _p(out))
     vt = torch.tensor(v, requires_grad=True)
@@ -140,5 +143,33 @@ def test_grid_bc_forward_and_adjoint(lib, mu):
     gv = np.zeros((n, 3))
     gmu = np.zeros(n)
     lib.h_grid_bc_bwd(n, _p(v), ijk.ctypes.data_as(_int), G, bound, ctypes.c_double(mu), _p(gout), _p(gv), _p(gmu))
-    np.testing.assert_allclose(gv, vt.grad.numpy(), rtol=1e-9, atol=1e-9)
-    assert gmu.sum() == pytest.approx(float(mut.grad), rel=1e-9, abs=1e-12)
+    assert np.isfinite(gv).all() and np.isfinite(gmu).all()
+    ok = np.isfinite(vt.grad.numpy()).all(axis=1)
+    np.testing.assert_allclose(gv[ok], vt.grad.numpy()[ok], rtol=1e-9, atol=1e-9)
+    if np.isfinite(float(mut.grad)):
+        assert gmu.sum() == pytest.approx(float(mut.grad), rel=1e-9, abs=1e-12)
+
+
+@pytest.mark.parametrize("mode", ["exact", "reference"])
+def test_float_stress_keeps_precision_at_small_strain(lib, mode):
+    """Cloth strains are ~1e-5..1e-3: the float build, fed F - I, must keep
+    near-float relative precision in P and in dL/d(mu, la) instead of losing it
+    to cancellation of O(1) numbers."""
+    n = 64
+    rng = np.random.default_rng(7)
+    F = np.eye(3)[None] + 1e-4 * rng.standard_normal((n, 3, 3))
+    F[: n // 2, 2, 2] -= 3e-4                      # normal compression: contact branch
+    E0, nu0, ks0, kc0 = 5e3, 0.3, 120.0, 340.0
+    mu, la = _mu_la(E0, nu0)
+    prm = np.tile([mu, la, ks0, kc0], (n, 1)).astype(np.float64)
+    Pd = np.zeros((n, 3, 3)); Pf = np.zeros((n, 3, 3))
+    lib.h_stress_fwd(n, 1, _p(np.ascontiguousarray(F)), _p(prm), _p(Pd))
+    lib.h_stress_fwd(n, 0, _p(np.ascontiguousarray(F)), _p(prm), _p(Pf))
+    assert np.abs(Pf - Pd).max() <= 2e-5 * np.abs(Pd).max()
+    gP = rng.standard_normal((n, 3, 3))
+    gd = np.zeros((n, 4)); gf = np.zeros((n, 4)); gF = np.zeros((n, 3, 3))
+    m = 0 if mode == "exact" else 1
+    lib.h_stress_bwd(n, 1, _p(np.ascontiguousarray(F)), _p(prm), _p(gP), m, _p(gF), _p(gd))
+    lib.h_stress_bwd(n, 0, _p(np.ascontiguousarray(F)), _p(prm), _p(gP), m, _p(gF), _p(gf))
+    for j in range(4):
+        assert abs(gf[:, j].sum() - gd[:, j].sum()) <= 1e-5 * np.abs(gd[:, j]).sum() + 1e-30, j

@@ -16,7 +16,7 @@ HEADER = os.path.join(ROOT, "include", "diffcp_b200.h")
 
 def declared_functions():
     txt = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|int64_t|const char\*)\s+(dcp_\w+)\s*\(", txt, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|int32_t|int64_t|const char\*)\s+(dcp_\w+)\s*\(", txt, re.M)))
 
 
 def test_library_loads_and_exports_every_declared_symbol():
