@@ -148,15 +148,15 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel, units):
-    """DRAM bytes per particle of ``kernel`` from the committed ncu summary
-    (profiles/<kernel>.md, line 'dram_bytes_per_particle: X'), scaled to a
-    launch of ``units`` particles; None when no summary exists."""
+def ncu_traffic(kernel):
+    """DRAM read + write bytes of one launch of ``kernel`` on this workload,
+    from the committed ncu summary (profiles/<kernel>.md, line
+    'dram_bytes_per_launch: X'); None when no summary exists."""
     path = os.path.join(ROOT, "profiles", kernel + ".md")
     if not os.path.exists(path):
         return None
-    m = re.search(r"dram_bytes_per_particle:\s*([0-9.eE+-]+)", open(path).read())
-    return float(m.group(1)) * units if m else None
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+-]+)", open(path).read())
+    return float(m.group(1)) if m else None
 
 
 def counts(scenes):
@@ -366,7 +366,7 @@ def main():
     avg_s = dms / dn / 1e3
     peak, peak_kind = peaks()
     achieved = alg / avg_s / 1e9 if alg else None
-    traffic = ncu_traffic(dname, units["tri"] if "tri" in per_unit else units["vertex"])
+    traffic = ncu_traffic(dname) if args.workload == "sweep" else None
     roof = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
             if peak_kind == "measured" else "fallback", "traffic": traffic, "alg_bytes_per_launch": alg,

@@ -36,8 +36,8 @@ class ClothBatch:
     returns data in the scenes' original order.
     """
 
-    def __init__(self, scenes: Sequence[ClothScene], dt: float, chunk: int = 128, tile_nodes: int = 2048,
-                 svd_grad: str = "exact", grid_ctas: int = 0, device=None, reorder: bool = True):
+    def __init__(self, scenes: Sequence[ClothScene], dt: float, chunk: int = 128, svd_grad: str = "exact",
+                 grid_ctas: int = 0, device=None, reorder: bool = True):
         self.device = torch.device(device if device is not None else "cuda")
         if self.device.type != "cuda":
             raise ValueError("diffcp_b200 runs on CUDA devices only")
@@ -81,8 +81,7 @@ class ClothBatch:
             I.gripper_radius = sc.gripper_radius
             I.n_traj_steps = 0 if sc.velocities is None else int(sc.velocities.shape[0])
         self._insts = insts
-        opt = DcpOptions(dt=self.dt, chunk=chunk, tile_nodes=tile_nodes, svd_grad=native.SVD_GRAD[svd_grad],
-                         grid_ctas=grid_ctas)
+        opt = DcpOptions(dt=self.dt, chunk=chunk, svd_grad=native.SVD_GRAD[svd_grad], grid_ctas=grid_ctas)
         self._opt = opt
         sizes = DcpSizes()
         check(self.lib.dcp_plan(insts, n, ctypes.byref(opt), ctypes.byref(sizes)), "dcp_plan")

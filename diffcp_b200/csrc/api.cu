@@ -46,7 +46,6 @@ int validate(const DcpInstance* in, int n, const DcpOptions* opt) {
   if (!in || n <= 0) return fail(DCP_ERR_INVALID, "n_inst must be positive");
   if (!opt) return fail(DCP_ERR_INVALID, "options missing");
   if (opt->chunk < 32 || opt->chunk > 256 || opt->chunk % 32) return fail(DCP_ERR_INVALID, "chunk must be 32..256, multiple of 32");
-  if (opt->tile_nodes < 0 || opt->tile_nodes > 14000) return fail(DCP_ERR_INVALID, "tile_nodes out of range");
   if (!(opt->dt > 0.f)) return fail(DCP_ERR_INVALID, "dt must be positive");
   for (int i = 0; i < n; ++i) {
     const DcpInstance& I = in[i];
@@ -264,7 +263,6 @@ int dcp_create(const DcpInstance* inst, int32_t n_inst, const DcpOptions* opt, c
   B.vertex_rank = (const int*)(sd + L.off_rank);
   B.dt = opt->dt;
   B.svd_grad = opt->svd_grad;
-  B.tile_nodes = opt->tile_nodes;
   B.grid_pm = (float4*)(wd + L.off_pm);
   B.grid_v = (float4*)(wd + L.off_v);
   B.grid_adj = (float4*)(wd + L.off_adj);
@@ -283,7 +281,7 @@ int dcp_create(const DcpInstance* inst, int32_t n_inst, const DcpOptions* opt, c
   b->L.block = opt->chunk;
   b->L.grid_ctas = opt->grid_ctas > 0 ? opt->grid_ctas : 148 * 8;
   b->L.prof = &b->prof;
-  e = configure_kernels(B);
+  e = configure_kernels(B, b->L);
   if (e != cudaSuccess) {
     delete b;
     return cuda_fail(e, "dcp_create configure");
@@ -413,11 +411,11 @@ static int run_maybe_graph(DcpBatch* b, GraphCache& gc, const std::vector<long l
     b->prof.launches = before;
     cudaGraph_t g = nullptr;
     e = cudaStreamEndCapture(cs, &g);
-    if (eb != cudaSuccess) {
+    if (eb != cudaSuccess || e != cudaSuccess) {
       if (g) cudaGraphDestroy(g);
-      return cuda_fail(eb, "captured launch");
+      cudaGetLastError();  // a failed capture must not surface in a later, unrelated call
+      return cuda_fail(eb != cudaSuccess ? eb : e, eb != cudaSuccess ? "captured launch" : "end capture");
     }
-    if (e != cudaSuccess) return cuda_fail(e, "end capture");
     e = cudaGraphInstantiate(&gc.exec, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");

@@ -24,7 +24,7 @@ namespace dcp {
 
 enum ChunkKind { CHUNK_VERTEX = 0, CHUNK_OPERATOR = 1, CHUNK_CUBE = 2, CHUNK_TRI = 3 };
 enum GripMode { GRIP_NONE = 0, GRIP_OPERATOR = 1, GRIP_KINEMATIC = 2 };
-enum Status { STATUS_OUT_OF_DOMAIN = 1, STATUS_NONFINITE = 2, STATUS_TILE_FALLBACK = 4 };
+enum Status { STATUS_OUT_OF_DOMAIN = 1, STATUS_NONFINITE = 2 };
 enum GridMode { GRID_FORWARD = 0, GRID_RECOMPUTE = 1 };
 
 // Parameter table row (floats): E, nu, shearing k_s, contact k_c, ground friction, damping.
@@ -60,7 +60,6 @@ struct BatchDev {
   const int* vertex_rank;  // [nv] tie-break rank for the Chamfer argmin
   float dt;
   int svd_grad;
-  int tile_nodes;  // shared-memory tile capacity (float4 nodes)
   // workspace
   float4* grid_pm;
   float4* grid_v;
@@ -157,101 +156,75 @@ __device__ __forceinline__ void mark_block(long long node, unsigned* flags, int*
   }
 }
 
-// ------------------------------------------------------------------ tiles
-// A CTA scatters its particles' 27-node stencils into a shared-memory tile
-// that covers the bounding box of the CTA's stencils, then flushes the tile to
-// the global grid with one vector atomic per touched node.  Particles of one
-// CTA are a contiguous, spatially coherent range of one instance (mesh order),
-// so the box is compact; when it exceeds the tile capacity the CTA falls back
-// to direct global atomics.
-struct TileHdr {
-  int lo[3];
-  int dim[3];
-  int vol;
-  int use;
-  int any;
-};
-
-__device__ __forceinline__ void tile_setup(TileHdr& T, const int base[3], bool valid, int capacity) {
-  __shared__ int red[6][32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-  int v[6];
+// ------------------------------------------------------------ warp scatter
+// Particle-centric scatter of 27-node stencils with warp aggregation.  The
+// particles of a chunk are in Morton order at cell granularity, so particles
+// sharing a base cell sit in consecutive lanes.  Each run of equal base cells
+// is reduced with shuffles (exact float32 sums, as many shuffle rounds as the
+// longest run needs) and only the run's first lane issues the vector atomic
+// (red.global.add.v4.f32, resolved in L2) for each of the 27 nodes.  MARK also
+// registers the (at most 8) grid blocks the run's stencil touches as active.
+// Every lane of the warp must call it; lanes without a particle pass
+// valid = false.
+template <bool MARK, class F>
+__device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I, int inst, const int base[3],
+                                             bool valid, F&& contrib) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int key = valid ? ((base[0] << 22) | (base[1] << 11) | base[2]) : -1 - lane;
+  const int prev = __shfl_up_sync(FULL, key, 1);
+  const bool head = lane == 0 || key != prev;
+  const unsigned hm = __ballot_sync(FULL, head);
+  const int seg = __popc(hm & (0xffffffffu >> (31 - lane)));
+  const unsigned after = lane == 31 ? 0u : (hm & (0xffffffffu << (lane + 1)));
+  const int run = head ? ((after ? __ffs(after) - 1 : 32) - lane) : 0;
+  const int maxrun = __reduce_max_sync(FULL, (unsigned)run);
+  const int rounds = maxrun <= 1 ? 0 : 32 - __clz(maxrun - 1);
+  bool same[5];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    v[a] = valid ? base[a] : 0x3fffffff;
-    v[3 + a] = valid ? base[a] : -0x3fffffff;
+  for (int r = 0; r < 5; ++r) {
+    const int d = 1 << r;
+    const int sg = __shfl_down_sync(FULL, seg, d);
+    same[r] = lane + d < 32 && sg == seg;
   }
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    v[a] = __reduce_min_sync(0xffffffffu, v[a]);
-    v[3 + a] = __reduce_max_sync(0xffffffffu, v[3 + a]);
-  }
-  if (lane == 0) {
-#pragma unroll
-    for (int a = 0; a < 6; ++a) red[a][warp] = v[a];
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int lo[3], hi[3];
-    for (int a = 0; a < 3; ++a) {
-      lo[a] = red[a][0];
-      hi[a] = red[3 + a][0];
-      for (int w = 1; w < nw; ++w) {
-        lo[a] = min(lo[a], red[a][w]);
-        hi[a] = max(hi[a], red[3 + a][w]);
-      }
-    }
-    T.any = hi[0] >= lo[0];
-    long long vol = 1;
-    for (int a = 0; a < 3; ++a) {
-      T.lo[a] = lo[a];
-      T.dim[a] = T.any ? hi[a] - lo[a] + 3 : 1;
-      vol *= T.dim[a];
-    }
-    T.use = T.any && vol <= capacity;
-    T.vol = T.use ? (int)vol : 0;
-  }
-  __syncthreads();
-}
-
-__device__ __forceinline__ void tile_zero(float4* tile, const TileHdr& T) {
-  for (int n = threadIdx.x; n < T.vol; n += blockDim.x) tile[n] = make_float4(0.f, 0.f, 0.f, 0.f);
-}
-
-// Add one node contribution (p.xyz, m) into the tile, or straight into the grid
-// when the CTA has no tile.  MARK registers the node's block as active.
-template <bool MARK>
-__device__ __forceinline__ void emit(float4* tile, const TileHdr& T, const BatchDev& B, const InstDev& I, int inst, int i,
-                                     int j, int k, float4 v) {
-  if (T.use) {
-    float* t = reinterpret_cast<float*>(tile + ((i - T.lo[0]) * T.dim[1] + (j - T.lo[1])) * T.dim[2] + (k - T.lo[2]));
-    atomicAdd(t + 0, v.x);
-    atomicAdd(t + 1, v.y);
-    atomicAdd(t + 2, v.z);
-    if (MARK) atomicAdd(t + 3, v.w);
-  } else {
-    const long long n = node_index(I, i, j, k);
-    float4* dst = (MARK ? B.grid_pm : B.grid_adj) + n;
-    atomicAdd(dst, v);
-    if (MARK && v.w != 0.f) mark_block(n, B.flags, B.list_blk, B.list_inst, B.counters, inst);
-  }
-}
-
-template <bool MARK>
-__device__ __forceinline__ void tile_flush(const float4* tile, const TileHdr& T, const BatchDev& B, const InstDev& I,
-                                           int inst) {
   float4* grid = MARK ? B.grid_pm : B.grid_adj;
-  const int d12 = T.dim[1] * T.dim[2];
-  for (int n = threadIdx.x; n < T.vol; n += blockDim.x) {
-    const float4 v = tile[n];
-    const bool nz = MARK ? (v.w != 0.f) : (v.x != 0.f || v.y != 0.f || v.z != 0.f);
-    if (nz) {
-      const int i = n / d12, r = n - i * d12, j = r / T.dim[2], k = r - j * T.dim[2];
-      const long long g = node_index(I, i + T.lo[0], j + T.lo[1], k + T.lo[2]);
-      atomicAdd(grid + g, v);
-      if (MARK) mark_block(g, B.flags, B.list_blk, B.list_inst, B.counters, inst);
-    }
+  if (MARK && head && valid) {
+#pragma unroll
+    for (int bi = 0; bi < 2; ++bi)
+#pragma unroll
+      for (int bj = 0; bj < 2; ++bj)
+#pragma unroll
+        for (int bk = 0; bk < 2; ++bk) {
+          const int i = base[0] + 2 * bi, j = base[1] + 2 * bj, k = base[2] + 2 * bk;
+          if ((bi && (i >> 2) == (base[0] >> 2)) || (bj && (j >> 2) == (base[1] >> 2)) ||
+              (bk && (k >> 2) == (base[2] >> 2)))
+            continue;
+          mark_block(node_index(I, i, j, k), B.flags, B.list_blk, B.list_inst, B.counters, inst);
+        }
   }
+#pragma unroll
+  for (int oi = 0; oi < 3; ++oi)
+#pragma unroll
+    for (int oj = 0; oj < 3; ++oj)
+#pragma unroll
+      for (int ok = 0; ok < 3; ++ok) {
+        float4 v = valid ? contrib(oi, oj, ok) : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int r = 0; r < rounds; ++r) {
+          const int d = 1 << r;
+          const float x = __shfl_down_sync(FULL, v.x, d);
+          const float y = __shfl_down_sync(FULL, v.y, d);
+          const float z = __shfl_down_sync(FULL, v.z, d);
+          const float w = __shfl_down_sync(FULL, v.w, d);
+          if (same[r]) {
+            v.x += x;
+            v.y += y;
+            v.z += z;
+            v.w += w;
+          }
+        }
+        if (head && valid && (v.x != 0.f || v.y != 0.f || v.z != 0.f || v.w != 0.f))
+          atomicAdd(grid + node_index(I, base[0] + oi, base[1] + oj, base[2] + ok), v);
+      }
 }
 
 // Warp + CTA sum of up to 8 doubles, one atomic per value per CTA.

@@ -66,7 +66,7 @@ struct LaunchCfg {
   Profiler* prof = nullptr;
 };
 
-cudaError_t configure_kernels(const BatchDev& B);
+cudaError_t configure_kernels(const BatchDev& B, const LaunchCfg& L);
 cudaError_t launch_init(const BatchDev& B, const LaunchCfg& L, const float* x0v, const float* x0o, const float* x0c,
                         float* state, float* rest, cudaStream_t s);
 cudaError_t launch_forward(const BatchDev& B, const LaunchCfg& L, const float* params, const float* traj, const float* rest,

@@ -161,41 +161,35 @@ __device__ __forceinline__ void lame(float E, float nu, float& mu, float& la) {
 // ============================================================== forward
 __global__ void __launch_bounds__(256) k_tri_forward(BatchDev B, const float* __restrict__ params,
                                                      const float* __restrict__ rest, const float* __restrict__ sin) {
-  extern __shared__ float4 tile[];
-  __shared__ TileHdr T;
   const Chunk ch = B.chunks[blockIdx.x];
   const InstDev& I = B.inst[ch.inst];
-  const bool valid = threadIdx.x < ch.count;
-  const long long t = ch.start + threadIdx.x;
+  const int tid = threadIdx.x;
+  const bool valid = tid < ch.count;
+  const long long t = ch.start + tid;
   const long long nt = B.nt;
   StateP S = state_ptrs(const_cast<float*>(sin), B.nv, B.nt, B.no);
   const RestP R = rest_ptrs(rest, B.nv, B.nt, B.no);
-  TriGeom g;
   Sten st;
+  float mv[3] = {0.f, 0.f, 0.f}, A[9], cP3[3] = {0.f, 0.f, 0.f}, d3[3] = {0.f, 0.f, 0.f};
+  const float m = I.m_q;
   if (valid) {
+    TriGeom g;
     load_tri(B, S, R, t, true, g);
     make_stencil(g.xc, I, st, B.status, ch.inst);
-  }
-  tile_setup(T, st.base, valid, B.tile_nodes);
-  if (!T.use && T.any && threadIdx.x == 0) atomicOr(B.status + ch.inst, STATUS_TILE_FALLBACK);
-  tile_zero(tile, T);
-  __syncthreads();
-  if (valid) {
     const float* prm = params + ch.inst * PRM_STRIDE;
     float mu, la;
     lame(prm[PRM_E], prm[PRM_NU], mu, la);
     const float ks = prm[PRM_KS], kc = prm[PRM_KC];
-    float C[9], dl3[3], n0[3], Di[9];
+    float dl3[3], n0[3], Di[9];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) C[q] = __ldg(S.t + q * nt + t);
+    for (int q = 0; q < 9; ++q) A[q] = __ldg(S.t + q * nt + t) * m;
     load_tri_rest(B, R, S, t, dl3, n0, Di);
     M3<float> d, Fe;
     tri_F(g, dl3, n0, Di, d, Fe);
-    const float d3[3] = {d.m[2], d.m[5], d.m[8]};
     Stress<float> sts;
     stress_forward<float>(Fe, mu, la, ks, kc, sts);
     const M3<float>& P = sts.P;
-    const float vol = I.vol_q, dt = B.dt, m = I.m_q, dx = I.dx, inv_dx = I.inv_dx;
+    const float vol = I.vol_q, dt = B.dt;
     // per-corner in-plane forces with r1 = (D0^-1[0,0], d[0,1], d[0,2]),
     // r2 = (D0^-1[1,0], d[1,1], d[1,2]) as in simulation.py:247-248
     const V3<float> r1 = v3(Di[0], d.m[1], d.m[2]);
@@ -208,35 +202,31 @@ __global__ void __launch_bounds__(256) k_tri_forward(BatchDev B, const float* __
     B.force[0 * e3 + 0 * nt + t] = f1.x; B.force[1 * e3 + 0 * nt + t] = f1.y; B.force[2 * e3 + 0 * nt + t] = f1.z;
     B.force[0 * e3 + 1 * nt + t] = f2.x; B.force[1 * e3 + 1 * nt + t] = f2.y; B.force[2 * e3 + 1 * nt + t] = f2.z;
     B.force[0 * e3 + 2 * nt + t] = f3.x; B.force[1 * e3 + 2 * nt + t] = f3.y; B.force[2 * e3 + 2 * nt + t] = f3.z;
-    // own-node APIC momentum + normal force (simulation.py:250-265)
-    const float mvx = m * g.vc[0], mvy = m * g.vc[1], mvz = m * g.vc[2];
-    float A[9];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) A[q] = C[q] * m;
     const float cn = -vol * dt;
-    const float P3x = P.m[2], P3y = P.m[5], P3z = P.m[8];
 #pragma unroll
-    for (int oi = 0; oi < 3; ++oi)
-#pragma unroll
-      for (int oj = 0; oj < 3; ++oj)
-#pragma unroll
-        for (int ok = 0; ok < 3; ++ok) {
-          const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
-          const float gx = st.dw[0][oi] * inv_dx * st.w[1][oj] * st.w[2][ok];
-          const float gy = st.w[0][oi] * (st.dw[1][oj] * inv_dx) * st.w[2][ok];
-          const float gz = st.w[0][oi] * st.w[1][oj] * (st.dw[2][ok] * inv_dx);
-          const float px = ((float)oi - st.fx[0]) * dx, py = ((float)oj - st.fx[1]) * dx, pz = ((float)ok - st.fx[2]) * dx;
-          const float nrm = cn * (gx * d3[0] + gy * d3[1] + gz * d3[2]);
-          float4 val;
-          val.x = W * (mvx + (A[0] * px + A[1] * py + A[2] * pz)) + nrm * P3x;
-          val.y = W * (mvy + (A[3] * px + A[4] * py + A[5] * pz)) + nrm * P3y;
-          val.z = W * (mvz + (A[6] * px + A[7] * py + A[8] * pz)) + nrm * P3z;
-          val.w = W * m;
-          emit<true>(tile, T, B, I, ch.inst, st.base[0] + oi, st.base[1] + oj, st.base[2] + ok, val);
-        }
+    for (int a = 0; a < 3; ++a) {
+      mv[a] = m * g.vc[a];
+      cP3[a] = cn * P.m[3 * a + 2];
+      d3[a] = d.m[3 * a + 2];
+    }
   }
-  __syncthreads();
-  if (T.use) tile_flush<true>(tile, T, B, I, ch.inst);
+  const float dx = I.dx, inv_dx = I.inv_dx;
+  // own-node APIC momentum, mass and normal force (simulation.py:250-265)
+  warp_scatter<true>(B, I, ch.inst, st.base, valid, [=](int oi, int oj, int ok) -> float4 {
+    const float w0 = st.w[0][oi], w1 = st.w[1][oj], w2 = st.w[2][ok];
+    const float W = w0 * w1 * w2;
+    const float gx = st.dw[0][oi] * inv_dx * w1 * w2;
+    const float gy = w0 * (st.dw[1][oj] * inv_dx) * w2;
+    const float gz = w0 * w1 * (st.dw[2][ok] * inv_dx);
+    const float px = ((float)oi - st.fx[0]) * dx, py = ((float)oj - st.fx[1]) * dx, pz = ((float)ok - st.fx[2]) * dx;
+    const float nrm = gx * d3[0] + gy * d3[1] + gz * d3[2];
+    float4 val;
+    val.x = W * (mv[0] + (A[0] * px + A[1] * py + A[2] * pz)) + nrm * cP3[0];
+    val.y = W * (mv[1] + (A[3] * px + A[4] * py + A[5] * pz)) + nrm * cP3[1];
+    val.z = W * (mv[2] + (A[6] * px + A[7] * py + A[8] * pz)) + nrm * cP3[2];
+    val.w = W * m;
+    return val;
+  });
 }
 
 __device__ __forceinline__ void point_arrays(const BatchDev& B, const StateP& S, int kind, float*& base, long long& n) {
@@ -267,32 +257,25 @@ __device__ __forceinline__ bool operator_velocity(const BatchDev& B, const InstD
 
 __global__ void __launch_bounds__(256) k_point_p2g(BatchDev B, const float* __restrict__ traj, int step, int window,
                                                    const float* __restrict__ rest, const float* __restrict__ sin) {
-  extern __shared__ float4 tile[];
-  __shared__ TileHdr T;
   const Chunk ch = B.chunks[B.n_tri_chunks + blockIdx.x];
   const InstDev& I = B.inst[ch.inst];
-  const bool valid = threadIdx.x < ch.count;
-  const long long p = ch.start + threadIdx.x;
+  const int tid = threadIdx.x;
+  const bool valid = tid < ch.count;
+  const long long p = ch.start + tid;
   StateP S = state_ptrs(const_cast<float*>(sin), B.nv, B.nt, B.no);
   float* arr;
   long long n;
   point_arrays(B, S, ch.kind, arr, n);
   const float* x0 = point_rest(rest_ptrs(rest, B.nv, B.nt, B.no), ch.kind);
-  float X[3];
+  const float m = ch.kind == CHUNK_VERTEX ? I.m_v : (ch.kind == CHUNK_OPERATOR ? I.m_o : I.m_c);
   Sten st;
+  float base_v[3] = {0.f, 0.f, 0.f}, A[9];
   if (valid) {
+    float X[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) X[a] = __ldg(x0 + a * n + p) + __ldg(arr + a * n + p);
     make_stencil(X, I, st, B.status, ch.inst);
-  }
-  tile_setup(T, st.base, valid, B.tile_nodes);
-  if (!T.use && T.any && threadIdx.x == 0) atomicOr(B.status + ch.inst, STATUS_TILE_FALLBACK);
-  tile_zero(tile, T);
-  __syncthreads();
-  if (valid) {
-    float m, base_v[3] = {0.f, 0.f, 0.f};
     if (ch.kind == CHUNK_VERTEX) {
-      m = I.m_v;
       float f[3] = {0.f, 0.f, 0.f};
       const long long e3 = 3LL * B.nt;
       const int e0 = __ldg(B.inc_ptr + p), e1 = __ldg(B.inc_ptr + p + 1);
@@ -306,36 +289,25 @@ __global__ void __launch_bounds__(256) k_point_p2g(BatchDev B, const float* __re
       base_v[1] = m * (__ldg(arr + 4 * n + p) + I.gravity_dv) + f[1];
       base_v[2] = m * __ldg(arr + 5 * n + p) + f[2];
     } else if (ch.kind == CHUNK_OPERATOR) {
-      m = I.m_o;
       float v[3];
       long long i0, i1;
       operator_velocity(B, I, traj, step, window, p, v, i0, i1);
       base_v[0] = m * v[0]; base_v[1] = m * v[1]; base_v[2] = m * v[2];
-    } else {
-      m = I.m_c;  // cube: affine momentum only (simulation.py:150-152)
-    }
-    float A[9];
+    }  // cube: affine momentum only (simulation.py:150-152)
 #pragma unroll
     for (int q = 0; q < 9; ++q) A[q] = m * __ldg(arr + (6 + q) * n + p);
-    const float dx = I.dx;
-#pragma unroll
-    for (int oi = 0; oi < 3; ++oi)
-#pragma unroll
-      for (int oj = 0; oj < 3; ++oj)
-#pragma unroll
-        for (int ok = 0; ok < 3; ++ok) {
-          const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
-          const float px = ((float)oi - st.fx[0]) * dx, py = ((float)oj - st.fx[1]) * dx, pz = ((float)ok - st.fx[2]) * dx;
-          float4 val;
-          val.x = W * (base_v[0] + (A[0] * px + A[1] * py + A[2] * pz));
-          val.y = W * (base_v[1] + (A[3] * px + A[4] * py + A[5] * pz));
-          val.z = W * (base_v[2] + (A[6] * px + A[7] * py + A[8] * pz));
-          val.w = W * m;
-          emit<true>(tile, T, B, I, ch.inst, st.base[0] + oi, st.base[1] + oj, st.base[2] + ok, val);
-        }
   }
-  __syncthreads();
-  if (T.use) tile_flush<true>(tile, T, B, I, ch.inst);
+  const float dx = I.dx;
+  warp_scatter<true>(B, I, ch.inst, st.base, valid, [=](int oi, int oj, int ok) -> float4 {
+    const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
+    const float px = ((float)oi - st.fx[0]) * dx, py = ((float)oj - st.fx[1]) * dx, pz = ((float)ok - st.fx[2]) * dx;
+    float4 val;
+    val.x = W * (base_v[0] + (A[0] * px + A[1] * py + A[2] * pz));
+    val.y = W * (base_v[1] + (A[3] * px + A[4] * py + A[5] * pz));
+    val.z = W * (base_v[2] + (A[6] * px + A[7] * py + A[8] * pz));
+    val.w = W * m;
+    return val;
+  });
 }
 
 // Node coordinates of lane l (0..63) of an active block.
@@ -522,50 +494,38 @@ __global__ void __launch_bounds__(256) k_g2p_adj(BatchDev B, const float* __rest
                                                  const float* __restrict__ rest, const float* __restrict__ sin,
                                                  const float* __restrict__ aout, float* __restrict__ ain,
                                                  double* __restrict__ gparams) {
-  extern __shared__ float4 tile[];
-  __shared__ TileHdr T;
   const Chunk ch = B.chunks[blockIdx.x];
   const InstDev& I = B.inst[ch.inst];
-  const bool valid = threadIdx.x < ch.count;
+  const int tid = threadIdx.x;
+  const bool valid = tid < ch.count;
   StateP Si = state_ptrs(const_cast<float*>(sin), B.nv, B.nt, B.no);
   StateP Ao = state_ptrs(const_cast<float*>(aout), B.nv, B.nt, B.no);
   StateP Ai = state_ptrs(ain, B.nv, B.nt, B.no);
   const RestP R = rest_ptrs(rest, B.nv, B.nt, B.no);
   const float dt = B.dt, inv_dx = I.inv_dx;
   const bool tri = ch.kind == CHUNK_TRI;
-  const long long idx = ch.start + threadIdx.x;
-  float X[3];
-  TriGeom g;
+  const long long idx = ch.start + tid;
   Sten st;
-  float *ai = nullptr, *ao = nullptr, *aa = nullptr;
-  long long n = 0;
-  if (!tri) {
-    point_arrays(B, Si, ch.kind, ai, n);
-    point_arrays(B, Ao, ch.kind, ao, n);
-    point_arrays(B, Ai, ch.kind, aa, n);
-  }
+  float gdamp[1] = {0.f};
+  float bV[3] = {0.f, 0.f, 0.f}, cbC[9];  // dL/dv' and 4 inv_dx dL/dC of the gather
   if (valid) {
+    float X[3];
+    float *ai = nullptr, *ao = nullptr, *aa = nullptr;
+    long long n = 0;
     if (tri) {
+      TriGeom g;
       load_tri(B, Si, R, idx, false, g);
       X[0] = g.xc[0]; X[1] = g.xc[1]; X[2] = g.xc[2];
     } else {
+      point_arrays(B, Si, ch.kind, ai, n);
+      point_arrays(B, Ao, ch.kind, ao, n);
+      point_arrays(B, Ai, ch.kind, aa, n);
       const float* x0 = point_rest(R, ch.kind);
 #pragma unroll
       for (int a = 0; a < 3; ++a) X[a] = __ldg(x0 + a * n + idx) + __ldg(ai + a * n + idx);
     }
     make_stencil(X, I, st, B.status, ch.inst);
-  }
-  tile_setup(T, st.base, valid, B.tile_nodes);
-  tile_zero(tile, T);
-  __syncthreads();
-  float gdamp[1] = {0.f};
-  if (valid) {
-    // gather the grid velocities of the stencil once
-    float3 gn[27];
-#pragma unroll
-    for (int q = 0; q < 27; ++q) gn[q] = gv(B, I, st.base[0] + q / 9, st.base[1] + (q / 3) % 3, st.base[2] + q % 3);
     float bC[9];  // adjoint of the gathered C (4 inv_dx sum W g (x) dpos)
-    float bV[3] = {0.f, 0.f, 0.f};
     float bx[3] = {0.f, 0.f, 0.f};
     if (tri) {
       const long long nt = B.nt;
@@ -575,7 +535,8 @@ __global__ void __launch_bounds__(256) k_g2p_adj(BatchDev B, const float* __rest
         const int oi = q / 9, oj = (q / 3) % 3, ok = q % 3;
         const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
         const float dp[3] = {(float)oi - st.fx[0], (float)oj - st.fx[1], (float)ok - st.fx[2]};
-        const float ga[3] = {gn[q].x, gn[q].y, gn[q].z};
+        const float3 gn = gv(B, I, st.base[0] + oi, st.base[1] + oj, st.base[2] + ok);
+        const float ga[3] = {gn.x, gn.y, gn.z};
         const float s = 4.f * W * inv_dx;
 #pragma unroll
         for (int a = 0; a < 3; ++a)
@@ -655,6 +616,7 @@ __global__ void __launch_bounds__(256) k_g2p_adj(BatchDev B, const float* __rest
 #pragma unroll
       for (int q = 0; q < 9; ++q) bC[q] = __ldg(ao + (6 + q) * n + idx);
     }
+    // position adjoint of the gather (second pass over the stencil)
     float px[3] = {0.f, 0.f, 0.f};
     const float c4 = 4.f * inv_dx;
 #pragma unroll
@@ -664,22 +626,16 @@ __global__ void __launch_bounds__(256) k_g2p_adj(BatchDev B, const float* __rest
       const float W = w0 * w1 * w2;
       const float gW[3] = {st.dw[0][oi] * w1 * w2 * inv_dx, w0 * st.dw[1][oj] * w2 * inv_dx, w0 * w1 * st.dw[2][ok] * inv_dx};
       const float dp[3] = {(float)oi - st.fx[0], (float)oj - st.fx[1], (float)ok - st.fx[2]};
-      const float ga[3] = {gn[q].x, gn[q].y, gn[q].z};
-      float bg[3];
+      const float3 gn = gv(B, I, st.base[0] + oi, st.base[1] + oj, st.base[2] + ok);
+      const float ga[3] = {gn.x, gn.y, gn.z};
       float s1 = bV[0] * ga[0] + bV[1] * ga[1] + bV[2] * ga[2];
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const float cd = bC[3 * a] * dp[0] + bC[3 * a + 1] * dp[1] + bC[3 * a + 2] * dp[2];
-        bg[a] = W * (bV[a] + c4 * cd);
-        s1 += c4 * ga[a] * cd;
-      }
+      for (int a = 0; a < 3; ++a) s1 += c4 * ga[a] * (bC[3 * a] * dp[0] + bC[3 * a + 1] * dp[1] + bC[3 * a + 2] * dp[2]);
 #pragma unroll
       for (int b = 0; b < 3; ++b) {
         const float cg = bC[b] * ga[0] + bC[3 + b] * ga[1] + bC[6 + b] * ga[2];
         px[b] += s1 * gW[b] - c4 * inv_dx * W * cg;
       }
-      emit<false>(tile, T, B, I, ch.inst, st.base[0] + oi, st.base[1] + oj, st.base[2] + ok,
-                  make_float4(bg[0], bg[1], bg[2], 0.f));
     }
     if (tri) {
       const long long nt = B.nt;
@@ -689,9 +645,20 @@ __global__ void __launch_bounds__(256) k_g2p_adj(BatchDev B, const float* __rest
 #pragma unroll
       for (int a = 0; a < 3; ++a) aa[a * n + idx] = bx[a] + px[a];
     }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) cbC[q] = c4 * bC[q];
   }
-  __syncthreads();
-  if (T.use) tile_flush<false>(tile, T, B, I, ch.inst);
+  // dL/dv_out at a node: W (dL/dv' + 4 inv_dx dL/dC dpos), dpos in cells
+  warp_scatter<false>(B, I, ch.inst, st.base, valid, [=](int oi, int oj, int ok) -> float4 {
+    const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
+    const float px = (float)oi - st.fx[0], py = (float)oj - st.fx[1], pz = (float)ok - st.fx[2];
+    float4 val;
+    val.x = W * (bV[0] + (cbC[0] * px + cbC[1] * py + cbC[2] * pz));
+    val.y = W * (bV[1] + (cbC[3] * px + cbC[4] * py + cbC[5] * pz));
+    val.z = W * (bV[2] + (cbC[6] * px + cbC[7] * py + cbC[8] * pz));
+    val.w = 0.f;
+    return val;
+  });
   if (tri) block_sum_atomic<1>(gdamp, gparams + ch.inst * PRM_STRIDE + PRM_DAMPING);
 }
 
@@ -847,7 +814,7 @@ __global__ void __launch_bounds__(256) k_point_adj(BatchDev B, const float* __re
 // force adjoints from dL/df of the three vertices, stress adjoint, and the
 // contributions to the three vertices (written per corner, summed by
 // k_vertex_collect).
-__global__ void __launch_bounds__(128) k_tri_adj(BatchDev B, const float* __restrict__ params,
+__global__ void __launch_bounds__(256) k_tri_adj(BatchDev B, const float* __restrict__ params,
                                                  const float* __restrict__ rest, const float* __restrict__ sin,
                                                  float* __restrict__ ain, double* __restrict__ gparams) {
   const Chunk ch = B.chunks[blockIdx.x];
@@ -1132,16 +1099,16 @@ cudaError_t launch_init(const BatchDev& B, const LaunchCfg& L, const float* x0v,
   return cudaGetLastError();
 }
 
-static inline size_t tile_bytes(const BatchDev& B) { return (size_t)B.tile_nodes * sizeof(float4); }
+
 
 cudaError_t launch_forward(const BatchDev& B, const LaunchCfg& L, const float* params, const float* traj, const float* rest,
                            int step, int window, const float* sin, float* sout, cudaStream_t s) {
   cudaMemsetAsync(B.counters, 0, sizeof(int), s);
   if (B.n_tri_chunks)
-    DCP_LAUNCH(KID_TRI_FORWARD, (k_tri_forward<<<B.n_tri_chunks, L.block, tile_bytes(B), s>>>(B, params, rest, sin)));
+    DCP_LAUNCH(KID_TRI_FORWARD, (k_tri_forward<<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin)));
   if (B.n_point_chunks)
     DCP_LAUNCH(KID_POINT_P2G,
-               (k_point_p2g<<<B.n_point_chunks, L.block, tile_bytes(B), s>>>(B, traj, step, window, rest, sin)));
+               (k_point_p2g<<<B.n_point_chunks, L.block, 0, s>>>(B, traj, step, window, rest, sin)));
   DCP_LAUNCH(KID_GRID, (k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_FORWARD)));
   DCP_LAUNCH(KID_G2P, (k_g2p<<<B.n_tri_chunks + B.n_point_chunks, L.block, 0, s>>>(B, params, rest, sin, sout)));
   return cudaGetLastError();
@@ -1152,12 +1119,12 @@ cudaError_t launch_backward(const BatchDev& B, const LaunchCfg& L, const float* 
                             double* gparams, double* gtraj, cudaStream_t s) {
   cudaMemsetAsync(B.counters, 0, sizeof(int), s);
   if (B.n_tri_chunks)
-    DCP_LAUNCH(KID_TRI_FORWARD, (k_tri_forward<<<B.n_tri_chunks, L.block, tile_bytes(B), s>>>(B, params, rest, sin)));
+    DCP_LAUNCH(KID_TRI_FORWARD, (k_tri_forward<<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin)));
   if (B.n_point_chunks)
     DCP_LAUNCH(KID_POINT_P2G,
-               (k_point_p2g<<<B.n_point_chunks, L.block, tile_bytes(B), s>>>(B, traj, step, window, rest, sin)));
+               (k_point_p2g<<<B.n_point_chunks, L.block, 0, s>>>(B, traj, step, window, rest, sin)));
   DCP_LAUNCH(KID_GRID, (k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_RECOMPUTE)));
-  DCP_LAUNCH(KID_G2P_ADJ, (k_g2p_adj<<<B.n_tri_chunks + B.n_point_chunks, L.block, tile_bytes(B), s>>>(
+  DCP_LAUNCH(KID_G2P_ADJ, (k_g2p_adj<<<B.n_tri_chunks + B.n_point_chunks, L.block, 0, s>>>(
                               B, params, rest, sin, aout, ain, gparams)));
   DCP_LAUNCH(KID_GRID_ADJ, (k_grid_adj<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, gparams, gtraj)));
   if (B.n_point_chunks)
@@ -1189,15 +1156,6 @@ cudaError_t launch_chamfer_backward(const BatchDev& B, const LaunchCfg& L, int m
   return cudaGetLastError();
 }
 
-cudaError_t configure_kernels(const BatchDev& B) {
-  const int bytes = (int)tile_bytes(B);
-  cudaError_t e = cudaSuccess;
-  if (bytes > 48 * 1024) {
-    e = cudaFuncSetAttribute(k_tri_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_point_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_g2p_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  }
-  return e;
-}
+cudaError_t configure_kernels(const BatchDev& B, const LaunchCfg& L) { return cudaSuccess; }
 
 }  // namespace dcp

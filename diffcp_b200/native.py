@@ -19,7 +19,7 @@ _fp = ctypes.POINTER(ctypes.c_float)
 DCP_OK = 0
 GRIP_NONE, GRIP_OPERATOR, GRIP_KINEMATIC = 0, 1, 2
 SVD_GRAD = {"exact": 0, "reference": 1}
-STATUS_OUT_OF_DOMAIN, STATUS_NONFINITE, STATUS_TILE_FALLBACK = 1, 2, 4
+STATUS_OUT_OF_DOMAIN, STATUS_NONFINITE = 1, 2
 
 EXPORTED = (
     "dcp_plan", "dcp_create", "dcp_destroy", "dcp_sizes", "dcp_init_state", "dcp_substep_forward",
@@ -42,8 +42,7 @@ class DcpInstance(ctypes.Structure):
 
 
 class DcpOptions(ctypes.Structure):
-    _fields_ = [("dt", c_float), ("chunk", c_int32), ("tile_nodes", c_int32), ("svd_grad", c_int32),
-                ("grid_ctas", c_int32)]
+    _fields_ = [("dt", c_float), ("chunk", c_int32), ("svd_grad", c_int32), ("grid_ctas", c_int32)]
 
 
 class DcpSizes(ctypes.Structure):

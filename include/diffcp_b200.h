@@ -61,7 +61,6 @@ extern "C" {
 
 #define DCP_STATUS_OUT_OF_DOMAIN 1 /* a stencil left the grid; clamped */
 #define DCP_STATUS_NONFINITE 2     /* a particle velocity became NaN/Inf */
-#define DCP_STATUS_TILE_FALLBACK 4 /* a CTA's stencils exceeded the shared-memory tile (performance only) */
 
 /* One cloth scene; the scalars are the constants of src/initialization.py:79,115-130. */
 typedef struct DcpInstance {
@@ -87,7 +86,6 @@ typedef struct DcpInstance {
 typedef struct DcpOptions {
   float dt;            /* substep (initialization.py:31) */
   int32_t chunk;       /* particles per CTA: multiple of 32 in [32, 256] */
-  int32_t tile_nodes;  /* shared-memory tile capacity in grid nodes (16 B each) */
   int32_t svd_grad;    /* DCP_SVD_GRAD_* */
   int32_t grid_ctas;   /* CTAs of the grid-update kernels, 0 = default */
 } DcpOptions;

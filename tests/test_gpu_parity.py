@@ -210,11 +210,22 @@ def test_graph_replay_equals_eager():
         np.testing.assert_allclose(o[1], out[0][1], rtol=1e-5, atol=1e-16)
 
 
-def test_tile_fallback_path_matches_tiled_path():
+@pytest.mark.parametrize("chunk", [32, 64, 256])
+def test_chunk_size_does_not_change_results(chunk):
     n = 12
-    sc = small_sheet(n_steps=n)
+    sc = small_sheet(n=9, n_steps=n)
     l1, g1, t1, _ = _sheet_grads(sc, n)
-    l2, g2, t2, b2 = _sheet_grads(sc, n, b=_batch([sc], tile_nodes=0))
+    l2, g2, t2, _ = _sheet_grads(sc, n, chunk=chunk)
+    assert float(l1[0]) == pytest.approx(float(l2[0]), rel=1e-6)
+    np.testing.assert_allclose(g1, g2, rtol=1e-5, atol=1e-16)
+    np.testing.assert_allclose(t1, t2, rtol=1e-5, atol=1e-5 * np.abs(t1).max())
+
+
+def test_unsorted_particle_order_matches_morton_order():
+    n = 12
+    sc = small_sheet(n=9, n_steps=n)
+    l1, g1, t1, _ = _sheet_grads(sc, n)
+    l2, g2, t2, _ = _sheet_grads(sc, n, reorder=False)
     assert float(l1[0]) == pytest.approx(float(l2[0]), rel=1e-6)
     np.testing.assert_allclose(g1, g2, rtol=1e-5, atol=1e-16)
 

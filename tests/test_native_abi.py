@@ -55,14 +55,14 @@ def _inst(**kw):
 def test_plan_sizes_and_validation():
     L = native.lib()
     insts = (native.DcpInstance * 2)(_inst(), _inst(n_grid=15, n_target=7))
-    opt = native.DcpOptions(dt=1e-4, chunk=128, tile_nodes=2048, svd_grad=0, grid_ctas=0)
+    opt = native.DcpOptions(dt=1e-4, chunk=128, svd_grad=0, grid_ctas=0)
     s = native.DcpSizes()
     assert L.dcp_plan(insts, 2, ctypes.byref(opt), ctypes.byref(s)) == 0
     assert s.n_vertex == 32 and s.n_tri == 36 and s.n_target == 7
     assert s.state_floats == 15 * 32 + 12 * 36
     assert s.total_nodes == 4 ** 3 * 64 * 2      # 15 nodes per axis pad to 4 blocks of 4
     assert s.n_tri_chunks == 2 and s.n_point_chunks == 2
-    bad = native.DcpOptions(dt=1e-4, chunk=100, tile_nodes=2048, svd_grad=0, grid_ctas=0)
+    bad = native.DcpOptions(dt=1e-4, chunk=100, svd_grad=0, grid_ctas=0)
     assert L.dcp_plan(insts, 2, ctypes.byref(bad), ctypes.byref(s)) == 1
     assert b"chunk" in L.dcp_last_error()
     insts2 = (native.DcpInstance * 1)(_inst(gripper_mode=1, n_grippers=2, group_size=3, n_operator=5, n_actions=4,
