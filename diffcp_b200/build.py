@@ -17,7 +17,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB_DIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIB_DIR, "libdiffcp_b200.so")
-SOURCES = ["kernels.cu", "api.cu"]
+SOURCES = ["kernels.cu", "api.cu", "chamfer_static.cu"]
 HEADERS = ["cloth_math.cuh", "dcp_internal.cuh", "dcp_launch.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -29,6 +29,14 @@ int cuda_fail(cudaError_t e, const char* where) {
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
+}  // namespace
+
+namespace dcp {
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace dcp
+
+namespace {
+
 struct Layout {
   std::vector<InstDev> inst;
   std::vector<Chunk> chunks;

@@ -26,7 +26,9 @@ EXPORTED = (
     "dcp_substep_backward", "dcp_chamfer_forward", "dcp_chamfer_backward", "dcp_rollout_floats",
     "dcp_rollout_state_offset", "dcp_rollout_forward", "dcp_rollout_backward", "dcp_read_status", "dcp_last_error",
     "dcp_launch_count", "dcp_profile", "dcp_profile_read", "dcp_kernel_count", "dcp_kernel_name",
+    "dcp_chamfer_forward_static",
 )
+STATIC_MAX_TARGETS = 1 << 20
 
 
 class DcpInstance(ctypes.Structure):
@@ -102,6 +104,8 @@ def lib():
     L.dcp_kernel_count.restype = c_int32
     L.dcp_kernel_name.argtypes = [c_int32]
     L.dcp_kernel_name.restype = ctypes.c_char_p
+    L.dcp_chamfer_forward_static.argtypes = [c_void_p, c_void_p, c_int32, c_void_p, c_int32, c_void_p, c_void_p,
+                                             c_void_p]
     for name in EXPORTED:
         getattr(L, name)
     _LIB = L

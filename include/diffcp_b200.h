@@ -183,6 +183,23 @@ int dcp_read_status(DcpBatch* batch, int32_t* host_status, int32_t clear, void* 
 
 const char* dcp_last_error(void);
 
+/* Chamfer loss of ONE cloth that allocates nothing -- no counterpart in the
+ * reference (compute_loss semantics, parameter_fitting_functions.py:3-15).
+ * For callers that cannot call cudaMalloc: a plugin whose host application's
+ * allocator owns the GPU's memory, or a latency-bound loop in which an
+ * allocation is not allowed.  The scratch (per-target minima) is a file-scope
+ * device array of DCP_STATIC_MAX_TARGETS floats that every GPU loading the
+ * library holds until exit.  The first call on a device, with that device
+ * current, looks up the array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU race.  x0, u (u may be NULL): [3][n_vertex]
+ * rest positions and displacements; targets: [3][n_target]; argmin:
+ * [n_target] vertex index (first index on ties); loss: one float.  Returns
+ * DCP_ERR_INVALID for n_target > DCP_STATIC_MAX_TARGETS. */
+#define DCP_STATIC_MAX_TARGETS (1 << 20)
+int dcp_chamfer_forward_static(const float* x0, const float* u, int32_t n_vertex, const float* targets,
+                               int32_t n_target, int32_t* argmin, float* loss, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
