@@ -239,6 +239,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-substeps", type=int, default=0,
                     help="run this many eager forward + adjoint substeps of the workload and exit (for ncu)")
+    ap.add_argument("--tune", action="store_true", help="autotune the launch configuration before timing")
+    ap.add_argument("--tune-cache", default=None, help="autotuner cache file (default diffcp_b200/tuned.json)")
+    ap.add_argument("--no-single", action="store_true", help="skip the single-instance plain-launch measurement")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -267,9 +270,17 @@ def main():
     dev = torch.device("cuda", torch.cuda.current_device())
     from diffcp_b200.batch import BatchSim, ClothBatch
 
+    from diffcp_b200 import autotune
     scenes, info = workload(args.workload, rank)
     nv, nt = counts(scenes)
-    batch = ClothBatch(scenes, dt=info["dt"], device=dev)
+    cache = args.tune_cache or autotune.CACHE
+    if args.tune:
+        launch = autotune.tune(scenes, info["dt"], device=dev, cache=cache, force=True)
+    else:
+        launch = autotune.cached(scenes, info["dt"], cache=cache) if os.path.exists(cache) else None
+        launch = launch or dict(autotune.DEFAULT, source="default")
+    batch = ClothBatch(scenes, dt=info["dt"], device=dev, chunk=launch["chunk"], scatter_mode=launch["scatter_mode"],
+                       min_blocks=launch["min_blocks"])
     sim = BatchSim(batch, n_steps=info["n_steps"], ckpt_every=info["ckpt_every"], use_graph=True)
     params = batch.params.clone().requires_grad_(True)
     traj = batch.traj.clone().requires_grad_(True)
@@ -376,6 +387,28 @@ def main():
     kernels = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / total_prof_ms, 4)}
                for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
 
+    # ---- the same work as single instances with plain per-kernel launches (no CUDA graph)
+    single = None
+    if not args.no_single and len(scenes) > 1:
+        sizes = [s_.n_vertex + s_.n_tri for s_ in scenes]
+        sc1 = scenes[int(np.argsort(sizes)[len(sizes) // 2])]
+        b1 = ClothBatch([sc1], dt=info["dt"], device=dev, chunk=launch["chunk"],
+                        scatter_mode=launch["scatter_mode"], min_blocks=launch["min_blocks"])
+        sim1 = BatchSim(b1, n_steps=info["n_steps"], ckpt_every=info["ckpt_every"], use_graph=False)
+        p1 = b1.params.clone().requires_grad_(True)
+        t1 = b1.traj.clone().requires_grad_(True)
+        sim1.loss(p1, t1).sum().backward()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        sim1.loss(p1, t1).sum().backward()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms1 = e0.elapsed_time(e1)
+        single = {"value": (sc1.n_vertex + sc1.n_tri) * info["n_steps"] / (ms1 / 1e3), "unit": UNIT,
+                  "ms_per_step": ms1, "instance": "%d vertices + %d triangles (median instance)" % (
+                      sc1.n_vertex, sc1.n_tri), "launches": "per-kernel launches, no CUDA graph"}
+        del sim1, b1
+
     if rank != 0:
         if world > 1:
             torch.distributed.destroy_process_group()
@@ -389,13 +422,15 @@ def main():
                    "substeps": info["n_steps"], "checkpoint_every": info["ckpt_every"],
                    "l2": "inputs larger than L2 (state snapshot %.0f MB, rollout buffer %.1f GB)"
                          % (batch.S * 4 / 1e6, sim._buf.numel() * 4 / 1e9),
-                   "parallelism": "independent instances per rank" if world > 1 else "one GPU"},
+                   "parallelism": "independent instances per rank" if world > 1 else "one GPU",
+                   "launch": launch},
         "roofline": roof,
         "step_roofline": {"achieved": step_alg / (ms_max / 1e3) / 1e9, "unit": "GB/s", "peak": peak,
                           "frac": step_alg / (ms_max / 1e3) / 1e9 / peak,
                           "bytes_per_particle": STEP_BYTES},
         "kernels": kernels,
         "cpu_baseline": cpu,
+        "single_instance": single,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": float(t.item())},
         "gpu_launches": int(launches),

@@ -55,6 +55,9 @@ int validate(const DcpInstance* in, int n, const DcpOptions* opt) {
   if (!opt) return fail(DCP_ERR_INVALID, "options missing");
   if (opt->chunk < 32 || opt->chunk > 256 || opt->chunk % 32) return fail(DCP_ERR_INVALID, "chunk must be 32..256, multiple of 32");
   if (!(opt->dt > 0.f)) return fail(DCP_ERR_INVALID, "dt must be positive");
+  if (opt->scatter_mode < 0 || opt->scatter_mode > 1) return fail(DCP_ERR_INVALID, "scatter_mode must be 0 or 1");
+  for (int k = 0; k < 3; ++k)
+    if (opt->min_blocks[k] < 0 || opt->min_blocks[k] > 3) return fail(DCP_ERR_INVALID, "min_blocks must be 0..3");
   for (int i = 0; i < n; ++i) {
     const DcpInstance& I = in[i];
     char buf[160];
@@ -271,6 +274,7 @@ int dcp_create(const DcpInstance* inst, int32_t n_inst, const DcpOptions* opt, c
   B.vertex_rank = (const int*)(sd + L.off_rank);
   B.dt = opt->dt;
   B.svd_grad = opt->svd_grad;
+  B.scatter_mode = opt->scatter_mode;
   B.grid_pm = (float4*)(wd + L.off_pm);
   B.grid_v = (float4*)(wd + L.off_v);
   B.grid_adj = (float4*)(wd + L.off_adj);
@@ -288,6 +292,8 @@ int dcp_create(const DcpInstance* inst, int32_t n_inst, const DcpOptions* opt, c
   B.total_blocks = L.total_nodes / 64;
   b->L.block = opt->chunk;
   b->L.grid_ctas = opt->grid_ctas > 0 ? opt->grid_ctas : 148 * 8;
+  const int default_minb[3] = {2, 2, 1};
+  for (int k = 0; k < 3; ++k) b->L.min_blocks[k] = opt->min_blocks[k] > 0 ? opt->min_blocks[k] : default_minb[k];
   b->L.prof = &b->prof;
   e = configure_kernels(B, b->L);
   if (e != cudaSuccess) {

@@ -60,6 +60,7 @@ struct BatchDev {
   const int* vertex_rank;  // [nv] tie-break rank for the Chamfer argmin
   float dt;
   int svd_grad;
+  int scatter_mode;  // 0: warp-aggregated runs, 1: one atomic per lane and node
   // workspace
   float4* grid_pm;
   float4* grid_v;
@@ -170,6 +171,35 @@ template <bool MARK, class F>
 __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I, int inst, const int base[3],
                                              bool valid, F&& contrib) {
   const unsigned FULL = 0xffffffffu;
+  float4* grid = MARK ? B.grid_pm : B.grid_adj;
+  if (B.scatter_mode == 1) {  // per-lane atomics: no shuffles, more L2 traffic
+    if (!valid) return;
+    if (MARK) {
+#pragma unroll
+      for (int bi = 0; bi < 2; ++bi)
+#pragma unroll
+        for (int bj = 0; bj < 2; ++bj)
+#pragma unroll
+          for (int bk = 0; bk < 2; ++bk) {
+            const int i = base[0] + 2 * bi, j = base[1] + 2 * bj, k = base[2] + 2 * bk;
+            if ((bi && (i >> 2) == (base[0] >> 2)) || (bj && (j >> 2) == (base[1] >> 2)) ||
+                (bk && (k >> 2) == (base[2] >> 2)))
+              continue;
+            mark_block(node_index(I, i, j, k), B.flags, B.list_blk, B.list_inst, B.counters, inst);
+          }
+    }
+#pragma unroll
+    for (int oi = 0; oi < 3; ++oi)
+#pragma unroll
+      for (int oj = 0; oj < 3; ++oj)
+#pragma unroll
+        for (int ok = 0; ok < 3; ++ok) {
+          const float4 v = contrib(oi, oj, ok);
+          if (v.x != 0.f || v.y != 0.f || v.z != 0.f || v.w != 0.f)
+            atomicAdd(grid + node_index(I, base[0] + oi, base[1] + oj, base[2] + ok), v);
+        }
+    return;
+  }
   const int lane = threadIdx.x & 31;
   const int key = valid ? ((base[0] << 22) | (base[1] << 11) | base[2]) : -1 - lane;
   const int prev = __shfl_up_sync(FULL, key, 1);
@@ -187,7 +217,6 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
     const int sg = __shfl_down_sync(FULL, seg, d);
     same[r] = lane + d < 32 && sg == seg;
   }
-  float4* grid = MARK ? B.grid_pm : B.grid_adj;
   if (MARK && head && valid) {
 #pragma unroll
     for (int bi = 0; bi < 2; ++bi)

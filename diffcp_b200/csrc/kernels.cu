@@ -159,7 +159,8 @@ __device__ __forceinline__ void lame(float E, float nu, float& mu, float& la) {
 }
 
 // ============================================================== forward
-__global__ void __launch_bounds__(256) k_tri_forward(BatchDev B, const float* __restrict__ params,
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_tri_forward(BatchDev B, const float* __restrict__ params,
                                                      const float* __restrict__ rest, const float* __restrict__ sin) {
   const Chunk ch = B.chunks[blockIdx.x];
   const InstDev& I = B.inst[ch.inst];
@@ -490,7 +491,8 @@ __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict
 // Reverse of k_g2p: scatter dL/dv_out into the adjoint grid and accumulate
 // the position adjoint of the gather; triangle: reverse of the d3 update and of
 // the skew/sym damping.
-__global__ void __launch_bounds__(256) k_g2p_adj(BatchDev B, const float* __restrict__ params,
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* __restrict__ params,
                                                  const float* __restrict__ rest, const float* __restrict__ sin,
                                                  const float* __restrict__ aout, float* __restrict__ ain,
                                                  double* __restrict__ gparams) {
@@ -814,7 +816,8 @@ __global__ void __launch_bounds__(256) k_point_adj(BatchDev B, const float* __re
 // force adjoints from dL/df of the three vertices, stress adjoint, and the
 // contributions to the three vertices (written per corner, summed by
 // k_vertex_collect).
-__global__ void __launch_bounds__(256) k_tri_adj(BatchDev B, const float* __restrict__ params,
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* __restrict__ params,
                                                  const float* __restrict__ rest, const float* __restrict__ sin,
                                                  float* __restrict__ ain, double* __restrict__ gparams) {
   const Chunk ch = B.chunks[blockIdx.x];
@@ -1085,6 +1088,10 @@ const char* const kKernelNames[KID_COUNT] = {
     "k_vertex_collect", "k_chamfer_fwd", "k_chamfer_loss", "k_chamfer_bwd", "k_init"};
 
 static inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+// Register-cap variants of the three register-heavy kernels: MINB resident
+// 256-thread CTAs per SM (1 = no cap).
+#define DCP_MINB(kernel, L, i) \
+  (L.min_blocks[i] >= 3 ? kernel<3> : (L.min_blocks[i] == 2 ? kernel<2> : kernel<1>))
 #define DCP_LAUNCH(id, ...)                   \
   do {                                        \
     ProfScope _scope(L.prof, (id), s);        \
@@ -1105,7 +1112,7 @@ cudaError_t launch_forward(const BatchDev& B, const LaunchCfg& L, const float* p
                            int step, int window, const float* sin, float* sout, cudaStream_t s) {
   cudaMemsetAsync(B.counters, 0, sizeof(int), s);
   if (B.n_tri_chunks)
-    DCP_LAUNCH(KID_TRI_FORWARD, (k_tri_forward<<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin)));
+    DCP_LAUNCH(KID_TRI_FORWARD, (DCP_MINB(k_tri_forward, L, 0)<<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin)));
   if (B.n_point_chunks)
     DCP_LAUNCH(KID_POINT_P2G,
                (k_point_p2g<<<B.n_point_chunks, L.block, 0, s>>>(B, traj, step, window, rest, sin)));
@@ -1119,19 +1126,19 @@ cudaError_t launch_backward(const BatchDev& B, const LaunchCfg& L, const float* 
                             double* gparams, double* gtraj, cudaStream_t s) {
   cudaMemsetAsync(B.counters, 0, sizeof(int), s);
   if (B.n_tri_chunks)
-    DCP_LAUNCH(KID_TRI_FORWARD, (k_tri_forward<<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin)));
+    DCP_LAUNCH(KID_TRI_FORWARD, (DCP_MINB(k_tri_forward, L, 0)<<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin)));
   if (B.n_point_chunks)
     DCP_LAUNCH(KID_POINT_P2G,
                (k_point_p2g<<<B.n_point_chunks, L.block, 0, s>>>(B, traj, step, window, rest, sin)));
   DCP_LAUNCH(KID_GRID, (k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_RECOMPUTE)));
-  DCP_LAUNCH(KID_G2P_ADJ, (k_g2p_adj<<<B.n_tri_chunks + B.n_point_chunks, L.block, 0, s>>>(
+  DCP_LAUNCH(KID_G2P_ADJ, (DCP_MINB(k_g2p_adj, L, 1)<<<B.n_tri_chunks + B.n_point_chunks, L.block, 0, s>>>(
                               B, params, rest, sin, aout, ain, gparams)));
   DCP_LAUNCH(KID_GRID_ADJ, (k_grid_adj<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, gparams, gtraj)));
   if (B.n_point_chunks)
     DCP_LAUNCH(KID_POINT_ADJ,
                (k_point_adj<<<B.n_point_chunks, L.block, 0, s>>>(B, traj, step, window, rest, sin, ain, gtraj)));
   if (B.n_tri_chunks)
-    DCP_LAUNCH(KID_TRI_ADJ, (k_tri_adj<<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin, ain, gparams)));
+    DCP_LAUNCH(KID_TRI_ADJ, (DCP_MINB(k_tri_adj, L, 2)<<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin, ain, gparams)));
   if (B.nv) DCP_LAUNCH(KID_VERTEX_COLLECT, (k_vertex_collect<<<ceil_div(B.nv, 256), 256, 0, s>>>(B, ain)));
   return cudaGetLastError();
 }

@@ -147,11 +147,13 @@ def reference_scene(args: dict, mesh_vertices, mesh_triangles, grasp_seq, target
     return sc
 
 
-def load_reference_scene(src_dir: str, seed: Optional[int] = None, args: Optional[dict] = None) -> ClothScene:
+def load_reference_scene(src_dir: str, seed: Optional[int] = None, args: Optional[dict] = None,
+                         seed_cube: Optional[int] = None) -> ClothScene:
     """Reads ``simulation_arguments.json`` in ``src_dir`` and the data files it
     names (initialization.py:26-77).  The reference draws its operator and cube
     clouds from unseeded generators; ``seed`` seeds them here (Python
-    ``random`` for the operator cloud, ``numpy.random`` for the cube cloud)."""
+    ``random`` for the operator cloud, ``numpy.random`` for the cube cloud,
+    which ``seed_cube`` can seed separately)."""
     if args is None:
         with open(os.path.join(src_dir, "simulation_arguments.json")) as fh:
             args = json.load(fh)
@@ -161,7 +163,7 @@ def load_reference_scene(src_dir: str, seed: Optional[int] = None, args: Optiona
     grasp = np.load(os.path.join(data, "grasp_traj_array.npy"))
     verts, tris = io_ply.read_ply(os.path.join(data, "cloth_mesh.ply"))
     n_c = args["rigid_cube_parameters"]["n_rigid_cube_particles"]
-    rs = np.random.RandomState(seed)
+    rs = np.random.RandomState(seed if seed_cube is None else seed_cube)
     cube_random = rs.rand(n_c, 3)
     n_op = args["operator_parameters"]["n_operator_particles"]
     group = int(n_op / grasp.shape[1])

@@ -49,3 +49,13 @@ def test_morton_order_is_a_permutation_and_local():
     assert sorted(order.tolist()) == list(range(len(v)))
     first = v[order[:16]]
     assert np.ptp(first[:, 0]) < 0.1 and np.ptp(first[:, 2]) < 0.1
+
+
+def test_reference_api_fails_loudly_without_cuda(tmp_path):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("checks the no-GPU error path")
+    from tests.ref_tree import write_tree
+    import diffcp_b200.reference_api as ref
+    with pytest.raises(RuntimeError, match="CUDA"):
+        ref.configure(write_tree(tmp_path), seed=0)
