@@ -242,6 +242,8 @@ def main():
     ap.add_argument("--tune", action="store_true", help="autotune the launch configuration before timing")
     ap.add_argument("--tune-cache", default=None, help="autotuner cache file (default diffcp_b200/tuned.json)")
     ap.add_argument("--no-single", action="store_true", help="skip the single-instance plain-launch measurement")
+    ap.add_argument("--no-tape", action="store_true",
+                    help="recompute particle-to-grid in every adjoint substep instead of restoring it from the grid tape")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -281,7 +283,8 @@ def main():
         launch = launch or dict(autotune.DEFAULT, source="default")
     batch = ClothBatch(scenes, dt=info["dt"], device=dev, chunk=launch["chunk"], scatter_mode=launch["scatter_mode"],
                        min_blocks=launch["min_blocks"])
-    sim = BatchSim(batch, n_steps=info["n_steps"], ckpt_every=info["ckpt_every"], use_graph=True)
+    tape = None if args.no_tape else "auto"
+    sim = BatchSim(batch, n_steps=info["n_steps"], ckpt_every=info["ckpt_every"], use_graph=True, tape=tape)
     params = batch.params.clone().requires_grad_(True)
     traj = batch.traj.clone().requires_grad_(True)
 
@@ -394,7 +397,7 @@ def main():
         sc1 = scenes[int(np.argsort(sizes)[len(sizes) // 2])]
         b1 = ClothBatch([sc1], dt=info["dt"], device=dev, chunk=launch["chunk"],
                         scatter_mode=launch["scatter_mode"], min_blocks=launch["min_blocks"])
-        sim1 = BatchSim(b1, n_steps=info["n_steps"], ckpt_every=info["ckpt_every"], use_graph=False)
+        sim1 = BatchSim(b1, n_steps=info["n_steps"], ckpt_every=info["ckpt_every"], use_graph=False, tape=tape)
         p1 = b1.params.clone().requires_grad_(True)
         t1 = b1.traj.clone().requires_grad_(True)
         sim1.loss(p1, t1).sum().backward()
@@ -409,6 +412,11 @@ def main():
                       sc1.n_vertex, sc1.n_tri), "launches": "per-kernel launches, no CUDA graph"}
         del sim1, b1
 
+    tape_info = None
+    if sim._tape is not None:
+        meta = ClothBatch.tape_blocks(sim._tape, info["n_steps"])
+        tape_info = {"bytes": int(sim._tape.numel()), "substeps_restored": int((meta[:, 0] >= 0).sum()),
+                     "active_blocks_per_substep": float(meta[:, 1].mean())}
     if rank != 0:
         if world > 1:
             torch.distributed.destroy_process_group()
@@ -423,7 +431,7 @@ def main():
                    "l2": "inputs larger than L2 (state snapshot %.0f MB, rollout buffer %.1f GB)"
                          % (batch.S * 4 / 1e6, sim._buf.numel() * 4 / 1e9),
                    "parallelism": "independent instances per rank" if world > 1 else "one GPU",
-                   "launch": launch},
+                   "launch": launch, "grid_tape": tape_info},
         "roofline": roof,
         "step_roofline": {"achieved": step_alg / (ms_max / 1e3) / 1e9, "unit": "GB/s", "peak": peak,
                           "frac": step_alg / (ms_max / 1e3) / 1e9 / peak,

@@ -187,6 +187,28 @@ class ClothBatch:
         return {"vx": v[0:3], "vv": v[3:6], "vC": v[6:15], "qC": t[0:9], "qd3": t[9:12], "ox": o[0:3],
                 "ov": o[3:6], "oC": o[6:15], "cx": c[0:3], "cv": c[3:6], "cC": c[6:15]}
 
+    def save_rest(self):
+        """Copies of the rest positions (vertices, operator, cube)."""
+        return self.x0_vertex.clone(), self.x0_operator.clone(), self.x0_cube.clone()
+
+    def restore_rest(self, saved) -> None:
+        self.x0_vertex.copy_(saved[0])
+        self.x0_operator.copy_(saved[1])
+        self.x0_cube.copy_(saved[2])
+
+    def rebase_rest(self, state: torch.Tensor) -> None:
+        """Make the positions of ``state`` the rest positions of the next
+        :meth:`init_state` (the reference's window carry-over,
+        parameter_fitting_functions.py:40-49: the end state's vertex, operator
+        and cube positions become the initial positions and the triangles'
+        rest shapes are rebuilt from them)."""
+        f = self.absolute_fields(state)
+        self.x0_vertex.copy_(f["vx"])
+        if self.no:
+            self.x0_operator.copy_(f["ox"])
+        if self.nc:
+            self.x0_cube.copy_(f["cx"])
+
     def new_state(self) -> torch.Tensor:
         return torch.zeros(self.S, dtype=torch.float32, device=self.device)
 
@@ -239,17 +261,34 @@ class ClothBatch:
             raise ValueError("state %d is not kept by a rollout with checkpoints every %d" % (step, ckpt_every))
         return buf[off: off + self.S]
 
-    def rollout_forward(self, buf, n_steps, ckpt_every, window=0, use_graph=True, params=None, traj=None):
+    def tape_buffer(self, n_steps: int, blocks: int) -> torch.Tensor:
+        """Grid tape for rollouts of n_steps substeps holding up to ``blocks``
+        active 4^3 node blocks in total (1 KB each)."""
+        nb = int(self.lib.dcp_tape_bytes(self.handle, n_steps, int(blocks)))
+        if nb < 0:
+            raise ValueError("bad tape size")
+        return torch.empty(nb, dtype=torch.uint8, device=self.device)
+
+    @staticmethod
+    def tape_blocks(tape: torch.Tensor, n_steps: int) -> np.ndarray:
+        """Per-substep (first slot or -1 when it did not fit, active blocks) of
+        the last forward rollout recorded into ``tape``."""
+        meta = tape[256: 256 + 8 * n_steps].view(torch.int32).reshape(n_steps, 2)
+        return meta.cpu().numpy()
+
+    def rollout_forward(self, buf, n_steps, ckpt_every, window=0, use_graph=True, params=None, traj=None, tape=None):
         check(self.lib.dcp_rollout_forward(self.handle, _ptr(self.params if params is None else params),
                                            _ptr(self.traj if traj is None else traj), _ptr(self.rest), window, n_steps,
-                                           ckpt_every, _ptr(buf), int(use_graph), _stream()), "dcp_rollout_forward")
+                                           ckpt_every, _ptr(buf), _ptr(tape), 0 if tape is None else tape.numel(),
+                                           int(use_graph), _stream()), "dcp_rollout_forward")
 
     def rollout_backward(self, buf, adj_work, n_steps, loss_step, ckpt_every, gparams, gtraj, window=0,
-                         use_graph=True, params=None, traj=None):
+                         use_graph=True, params=None, traj=None, tape=None):
         check(self.lib.dcp_rollout_backward(self.handle, _ptr(self.params if params is None else params),
                                             _ptr(self.traj if traj is None else traj), _ptr(self.rest), window,
                                             n_steps, loss_step, ckpt_every, _ptr(buf), _ptr(adj_work),
-                                            _ptr(gparams), _ptr(gtraj), int(use_graph), _stream()),
+                                            _ptr(gparams), _ptr(gtraj), _ptr(tape),
+                                            0 if tape is None else tape.numel(), int(use_graph), _stream()),
               "dcp_rollout_backward")
 
     def launch_count(self) -> int:
@@ -298,7 +337,10 @@ class _RolloutLoss(torch.autograd.Function):
         buf = sim._buffer(L, ckpt_every)
         s0 = b.state_in_buffer(buf, L, ckpt_every, 0)
         b.init_state(out=s0, x0_vertex=sim.x0_vertex)
-        b.rollout_forward(buf, L, ckpt_every, window=window, use_graph=use_graph, params=params, traj=traj)
+        tape = sim._tape_for(L)
+        b.rollout_forward(buf, L, ckpt_every, window=window, use_graph=use_graph, params=params, traj=traj,
+                          tape=tape)
+        sim._tape_sized(tape, L)
         sL = b.state_in_buffer(buf, L, ckpt_every, L)
         loss, arg = b.chamfer(sL, sim.targets)
         # substeps after the loss state carry no gradient (the reference's loss
@@ -310,7 +352,7 @@ class _RolloutLoss(torch.autograd.Function):
             cur = nxt
         sim.final_state = cur.clone() if n_steps > L else sL.clone()
         ctx.sim, ctx.L, ctx.K, ctx.window, ctx.use_graph = sim, L, ckpt_every, window, use_graph
-        ctx.buf, ctx.arg = buf, arg
+        ctx.buf, ctx.arg, ctx.tape = buf, arg, tape
         ctx.save_for_backward(params, traj)
         return loss
 
@@ -325,7 +367,7 @@ class _RolloutLoss(torch.autograd.Function):
         b.chamfer_backward(sL, ctx.arg, gloss.contiguous().float(), adj[0], sim.targets)
         gp, gt = b.new_grads()
         b.rollout_backward(ctx.buf, adj, L, L, K, gp, gt, window=ctx.window, use_graph=ctx.use_graph, params=params,
-                           traj=traj)
+                           traj=traj, tape=ctx.tape)
         sim.adj_state0 = adj[L % 2]
         return gp.to(params.dtype), gt[: traj.numel()].to(traj.dtype), None, None, None, None, None, None
 
@@ -336,10 +378,17 @@ class BatchSim:
     ``loss(params, traj)`` returns the per-instance loss (n_inst,), and
     ``backward()`` on it fills ``params.grad`` (n_inst, 8: dE, dnu,
     d shearing, d contact, d friction, d damping, 0, 0) and ``traj.grad``.
+
+    ``tape``: "auto" records each forward substep's particle-to-grid result so
+    that the adjoint restores it instead of recomputing P2G.  The first call
+    only counts the active blocks per substep (and recomputes); the tape is
+    then sized to ``tape_margin`` times that count.  Substeps that do not fit
+    (the cloth spread over more blocks later) recompute.  None disables it; an
+    int gives the capacity in blocks directly.
     """
 
     def __init__(self, batch: ClothBatch, n_steps: int, loss_step: Optional[int] = None, ckpt_every: int = 1,
-                 use_graph: bool = True):
+                 use_graph: bool = True, tape="auto", tape_margin: float = 1.25):
         self.batch = batch
         self.n_steps = int(n_steps)
         self.loss_step = self.n_steps if loss_step is None else int(loss_step)
@@ -353,6 +402,29 @@ class BatchSim:
         self._adj = torch.zeros(2, batch.S, dtype=torch.float32, device=batch.device)
         self.final_state = None
         self.adj_state0 = None
+        self.tape_mode = tape
+        self.tape_margin = float(tape_margin)
+        self._tape = None
+        self._tape_key = None
+
+    def _tape_for(self, L):
+        """The tape for a rollout of L substeps (None when disabled)."""
+        if self.tape_mode is None:
+            return None
+        if self._tape_key != L:
+            blocks = self.tape_mode if isinstance(self.tape_mode, int) else 0   # "auto": count first
+            self._tape = self.batch.tape_buffer(L, blocks)
+            self._tape_key = L
+            self._tape_counted = isinstance(self.tape_mode, int)
+        return self._tape
+
+    def _tape_sized(self, tape, L):
+        """After the counting rollout, replace the tape by one that fits."""
+        if tape is None or self._tape_counted:
+            return
+        counts = ClothBatch.tape_blocks(tape, L)[:, 1].astype(np.int64)
+        self._tape = self.batch.tape_buffer(L, int(np.ceil(counts.sum() * self.tape_margin)) + 64)
+        self._tape_counted = True
 
     def _buffer(self, L, K):
         if self._buf_key != (L, K):

@@ -342,6 +342,42 @@ int dcp_substep_forward(DcpBatch* b, const float* params, const float* traj, con
   return e == cudaSuccess ? DCP_OK : cuda_fail(e, "dcp_substep_forward");
 }
 
+int dcp_reset_quadrature(DcpBatch* b, float* rest, float* state, float* fdev, void* stream) {
+  if (!b || !rest || !state || (!fdev && b->B.nt)) return fail(DCP_ERR_INVALID, "NULL argument");
+  cudaError_t e = launch_reset(b->B, b->L, rest, state, fdev, (cudaStream_t)stream);
+  return e == cudaSuccess ? DCP_OK : cuda_fail(e, "dcp_reset_quadrature");
+}
+
+int dcp_replay(DcpBatch* b, const float* params, const float* traj, float* rest, float* state, float* work,
+               float* fdev, int32_t first_step, int32_t n_blocks, int32_t block_steps, int32_t fdev_pending,
+               void* stream) {
+  if (!b || !params || !rest || !state || !work || (!fdev && b->B.nt)) return fail(DCP_ERR_INVALID, "NULL argument");
+  if (state == work) return fail(DCP_ERR_INVALID, "state and work must differ");
+  if (first_step < 0 || n_blocks < 0 || block_steps < 1) return fail(DCP_ERR_INVALID, "bad replay counts");
+  cudaStream_t s = (cudaStream_t)stream;
+  float* cur = state;
+  float* nxt = work;
+  int step = first_step;
+  bool pending = fdev_pending != 0;
+  for (int blk = 0; blk < n_blocks; ++blk) {
+    for (int k = 0; k < block_steps; ++k, ++step) {
+      cudaError_t e = launch_forward(b->B, b->L, params, traj, rest, step, 0, cur, nxt, s, nullptr,
+                                     pending ? fdev : nullptr);
+      if (e != cudaSuccess) return cuda_fail(e, "dcp_replay");
+      pending = false;
+      std::swap(cur, nxt);
+    }
+    cudaError_t e = launch_reset(b->B, b->L, rest, cur, fdev, s);
+    if (e != cudaSuccess) return cuda_fail(e, "dcp_replay reset");
+    pending = true;
+  }
+  if (cur != state) {
+    cudaError_t e = cudaMemcpyAsync(state, cur, sizeof(float) * b->sizes.state_floats, cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(e, "dcp_replay copy");
+  }
+  return DCP_OK;
+}
+
 int dcp_substep_backward(DcpBatch* b, const float* params, const float* traj, const float* rest, int32_t step,
                          int32_t window, const float* sin, const float* aout, float* ain, double* gparams,
                          double* gtraj, void* stream) {
@@ -445,20 +481,61 @@ static int run_maybe_graph(DcpBatch* b, GraphCache& gc, const std::vector<long l
   return e == cudaSuccess ? DCP_OK : cuda_fail(e, "graph launch");
 }
 
+// Grid tape layout: [256 B header: int top][meta int2 n][fv float 3*nv*n]
+// [blk int cap][inst int cap][data float4 64*cap], each part 256-B aligned.
+static size_t tape_fixed(const DcpBatch* b, int n) {
+  return 256 + align256(8ull * n) + align256(12ull * n * b->lay.nv);
+}
+static size_t tape_size(const DcpBatch* b, int n, long long cap) {
+  return tape_fixed(b, n) + 2 * align256(4ull * cap) + 1024ull * cap;
+}
+
+// Carves the tape; returns false when it is too small for its fixed part.
+static bool tape_layout(const DcpBatch* b, int n, void* tape, long long bytes, TapeP& T) {
+  const size_t fixed = tape_fixed(b, n);
+  if (!tape || bytes < 0 || (size_t)bytes < fixed) return false;
+  long long cap = ((long long)bytes - (long long)fixed - 512) / 1032;
+  if (cap < 0) cap = 0;
+  while (cap > 0 && tape_size(b, n, cap) > (size_t)bytes) --cap;
+  char* p = (char*)tape;
+  T.top = (int*)p;
+  T.meta = (int2*)(p + 256);
+  T.fv = (float*)(p + 256 + align256(8ull * n));
+  T.blk = (int*)(p + fixed);
+  T.inst = (int*)(p + fixed + align256(4ull * cap));
+  T.data = (float4*)(p + fixed + 2 * align256(4ull * cap));
+  T.cap = std::min<long long>(cap, 0x7fffffffLL);
+  return true;
+}
+
 extern "C" {
 
+int64_t dcp_tape_bytes(const DcpBatch* b, int32_t n, int64_t blocks) {
+  if (!b || n < 0 || blocks < 0) return -1;
+  return (int64_t)tape_size(b, n, blocks);
+}
+
 int dcp_rollout_forward(DcpBatch* b, const float* params, const float* traj, const float* rest, int32_t window,
-                        int32_t n, int32_t K, float* buf, int32_t use_graph, void* stream) {
+                        int32_t n, int32_t K, float* buf, void* tape, int64_t tape_bytes, int32_t use_graph,
+                        void* stream) {
   if (!b || !params || !rest || !buf || n < 0 || K < 1) return fail(DCP_ERR_INVALID, "bad rollout arguments");
+  TapeP T;
+  if (tape && !tape_layout(b, n, tape, tape_bytes, T)) return fail(DCP_ERR_INVALID, "tape smaller than its fixed part");
   const long long S = b->sizes.state_floats;
   const long long seg0 = n_ckpt_slots(n, K) * S;
-  std::vector<long long> key = {(long long)params, (long long)traj, (long long)rest, (long long)buf, window, n, K};
+  std::vector<long long> key = {(long long)params, (long long)traj, (long long)rest, (long long)buf, window, n, K,
+                                (long long)tape, tape_bytes};
   return run_maybe_graph(b, b->gfwd, key, use_graph, stream, [&](cudaStream_t s) -> cudaError_t {
+    if (tape && n > 0) {
+      cudaError_t e = cudaMemsetAsync(T.top, 0, sizeof(int), s);
+      if (e == cudaSuccess) e = cudaMemsetAsync(T.meta, 0xff, 8ull * n, s);
+      if (e != cudaSuccess) return e;
+    }
     const float* cur = buf;
     for (int f = 0; f < n; ++f) {
       const long long slot = ckpt_slot(f + 1, n, K);
       float* nxt = slot >= 0 ? buf + slot * S : buf + seg0 + ((f + 1) % 2) * S;
-      cudaError_t e = launch_forward(b->B, b->L, params, traj, rest, f, window, cur, nxt, s);
+      cudaError_t e = launch_forward(b->B, b->L, params, traj, rest, f, window, cur, nxt, s, tape ? &T : nullptr);
       if (e != cudaSuccess) return e;
       cur = nxt;
     }
@@ -468,14 +545,18 @@ int dcp_rollout_forward(DcpBatch* b, const float* params, const float* traj, con
 
 int dcp_rollout_backward(DcpBatch* b, const float* params, const float* traj, const float* rest, int32_t window,
                          int32_t n, int32_t Lstep, int32_t K, float* buf, float* adj, double* gparams,
-                         double* gtraj, int32_t use_graph, void* stream) {
+                         double* gtraj, void* tape, int64_t tape_bytes, int32_t use_graph, void* stream) {
   if (!b || !params || !rest || !buf || !adj || !gparams || n < 0 || K < 1 || Lstep < 0 || Lstep > n)
     return fail(DCP_ERR_INVALID, "bad rollout arguments");
   if (b->sizes.traj_floats > 0 && (!traj || !gtraj)) return fail(DCP_ERR_INVALID, "trajectory buffers required");
+  TapeP T;
+  if (tape && !tape_layout(b, n, tape, tape_bytes, T)) return fail(DCP_ERR_INVALID, "tape smaller than its fixed part");
+  const TapeP* tp = tape ? &T : nullptr;
   const long long S = b->sizes.state_floats;
   const long long seg0 = n_ckpt_slots(n, K) * S;
   std::vector<long long> key = {(long long)params, (long long)traj, (long long)rest, (long long)buf, (long long)adj,
-                                (long long)gparams, (long long)gtraj, window, n, Lstep, K};
+                                (long long)gparams, (long long)gtraj, window, n, Lstep, K, (long long)tape,
+                                tape_bytes};
   return run_maybe_graph(b, b->gbwd, key, use_graph, stream, [&](cudaStream_t s) -> cudaError_t {
     if (Lstep == 0) return cudaSuccess;
     for (int seg = (Lstep - 1) / K; seg >= 0; --seg) {
@@ -489,7 +570,7 @@ int dcp_rollout_backward(DcpBatch* b, const float* params, const float* traj, co
       for (int f = last; f >= f0; --f) {
         const int so = (Lstep - 1 - f) % 2;
         cudaError_t e = launch_backward(b->B, b->L, params, traj, rest, f, window, state_at(f), adj + so * S,
-                                        adj + (1 - so) * S, gparams, gtraj, s);
+                                        adj + (1 - so) * S, gparams, gtraj, s, tp);
         if (e != cudaSuccess) return e;
       }
     }

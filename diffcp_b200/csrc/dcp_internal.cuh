@@ -93,6 +93,20 @@ __host__ __device__ inline StateP state_ptrs(float* base, int nv, int nt, int no
   return s;
 }
 
+// Grid tape of a rollout: per substep, the active blocks' (p, m) and every
+// vertex's summed corner force, so that the adjoint substep can restore the
+// grid instead of recomputing P2G.  Substeps that do not fit the block pool
+// are marked (meta.x = -1) and recomputed.
+struct TapeP {
+  int* top;        // [1] next free block slot
+  int2* meta;      // [n_steps] (first slot or -1, active block count)
+  int* blk;        // [cap] global block ids
+  int* inst;       // [cap] instances
+  float4* data;    // [cap][64] (p, m)
+  float* fv;       // [n_steps][3][nv] summed corner forces
+  long long cap;   // block capacity
+};
+
 struct RestP {
   const float* Di;  // [9][nt]
   const float* n0;  // [3][nt]

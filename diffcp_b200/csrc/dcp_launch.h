@@ -10,7 +10,7 @@ namespace dcp {
 
 enum KernelId {
   KID_TRI_FORWARD = 0, KID_POINT_P2G, KID_GRID, KID_G2P, KID_G2P_ADJ, KID_GRID_ADJ, KID_POINT_ADJ, KID_TRI_ADJ,
-  KID_VERTEX_COLLECT, KID_CHAMFER_FWD, KID_CHAMFER_LOSS, KID_CHAMFER_BWD, KID_INIT, KID_COUNT
+  KID_VERTEX_COLLECT, KID_CHAMFER_FWD, KID_CHAMFER_LOSS, KID_CHAMFER_BWD, KID_INIT, KID_TAPE, KID_RESET, KID_COUNT
 };
 extern const char* const kKernelNames[KID_COUNT];
 
@@ -70,11 +70,18 @@ struct LaunchCfg {
 cudaError_t configure_kernels(const BatchDev& B, const LaunchCfg& L);
 cudaError_t launch_init(const BatchDev& B, const LaunchCfg& L, const float* x0v, const float* x0o, const float* x0c,
                         float* state, float* rest, cudaStream_t s);
+// T (optional): the rollout's grid tape; forward substeps record into it,
+// adjoint substeps restore from it and skip the P2G recompute.
+// fdev (optional): F - I per triangle ([9][nt]) that replaces the one formed
+// from the state in this substep's stress (the substep after a replay reset).
 cudaError_t launch_forward(const BatchDev& B, const LaunchCfg& L, const float* params, const float* traj, const float* rest,
-                           int step, int window, const float* sin, float* sout, cudaStream_t s);
+                           int step, int window, const float* sin, float* sout, cudaStream_t s,
+                           const TapeP* T = nullptr, const float* fdev = nullptr);
+cudaError_t launch_reset(const BatchDev& B, const LaunchCfg& L, float* rest, float* state, float* fdev,
+                         cudaStream_t s);
 cudaError_t launch_backward(const BatchDev& B, const LaunchCfg& L, const float* params, const float* traj,
                             const float* rest, int step, int window, const float* sin, const float* aout, float* ain,
-                            double* gparams, double* gtraj, cudaStream_t s);
+                            double* gparams, double* gtraj, cudaStream_t s, const TapeP* T = nullptr);
 cudaError_t launch_chamfer_forward(const BatchDev& B, const LaunchCfg& L, int max_nq, const float* rest,
                                    const float* state, const float* targets, int* qarg, float* loss, cudaStream_t s);
 cudaError_t launch_chamfer_backward(const BatchDev& B, const LaunchCfg& L, int max_nq, const float* rest,

@@ -18,7 +18,13 @@
 //   k_g2p            G2P for all species + triangle state update
 //                    (simulation.py:304-430)
 // Reverse substep: k_g2p_adj, k_grid_adj, k_point_adj, k_tri_adj, k_vertex_collect.
+// Grid tape (optional): k_tape_reserve / k_tape_restore keep each forward
+// substep's particle-to-grid result so that the reverse substep skips P2G.
+// Replay (forward only, simulation_without_grad.py): k_reset_tri /
+// k_reset_vertex re-base the rest frames every few substeps.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include "dcp_internal.cuh"
 #include "dcp_launch.h"
@@ -34,6 +40,33 @@ __device__ __forceinline__ float3 ld3(const float* base, long long stride, long 
 // and affine matrices; rest positions x0; triangle rest normal n0 = the
 // normalised cross product of the eps-normalised edges (norm(1e-6)) and the
 // rest-shape inverse D0^-1 of D0 = [e1, e2, n0].
+// Rest frame of a triangle with corners pa, pb, pc: D0 = [pb - pa, pc - pa, n]
+// with n the normalised cross product of the eps-normalised edges (norm(1e-6)),
+// and D0^-1 by the adjugate (simulation.py:462-476, and the same frame in
+// reset_quadrature_particles of simulation_without_grad.py:471-485).
+__device__ __forceinline__ void rest_frame(const float pa[3], const float pb[3], const float pc[3], float inv[9],
+                                           float nrm[3]) {
+  const float d1x = pb[0] - pa[0], d1y = pb[1] - pa[1], d1z = pb[2] - pa[2];
+  const float d2x = pc[0] - pa[0], d2y = pc[1] - pa[1], d2z = pc[2] - pa[2];
+  const float l1 = sqrtf(d1x * d1x + d1y * d1y + d1z * d1z + 1e-6f);
+  const float l2 = sqrtf(d2x * d2x + d2y * d2y + d2z * d2z + 1e-6f);
+  const float n1x = d1x / l1, n1y = d1y / l1, n1z = d1z / l1;
+  const float n2x = d2x / l2, n2y = d2y / l2, n2z = d2z / l2;
+  float nx = n1y * n2z - n1z * n2y, ny = n1z * n2x - n1x * n2z, nz = n1x * n2y - n1y * n2x;
+  const float l3 = sqrtf(nx * nx + ny * ny + nz * nz + 1e-6f);
+  nx /= l3; ny /= l3; nz /= l3;
+  const float m00 = d1x, m01 = d2x, m02 = nx, m10 = d1y, m11 = d2y, m12 = ny, m20 = d1z, m21 = d2z, m22 = nz;
+  const float c00 = m11 * m22 - m12 * m21, c01 = m02 * m21 - m01 * m22, c02 = m01 * m12 - m02 * m11;
+  const float c10 = m12 * m20 - m10 * m22, c11 = m00 * m22 - m02 * m20, c12 = m02 * m10 - m00 * m12;
+  const float c20 = m10 * m21 - m11 * m20, c21 = m01 * m20 - m00 * m21, c22 = m00 * m11 - m01 * m10;
+  const float det = m00 * c00 + m01 * c10 + m02 * c20;
+  const float id = 1.f / det;
+  inv[0] = c00 * id; inv[1] = c01 * id; inv[2] = c02 * id;
+  inv[3] = c10 * id; inv[4] = c11 * id; inv[5] = c12 * id;
+  inv[6] = c20 * id; inv[7] = c21 * id; inv[8] = c22 * id;
+  nrm[0] = nx; nrm[1] = ny; nrm[2] = nz;
+}
+
 __global__ void k_init(BatchDev B, const float* __restrict__ x0v, const float* __restrict__ x0o,
                        const float* __restrict__ x0c, float* __restrict__ state, float* __restrict__ rest) {
   StateP S = state_ptrs(state, B.nv, B.nt, B.no);
@@ -56,31 +89,16 @@ __global__ void k_init(BatchDev B, const float* __restrict__ x0v, const float* _
     const long long t = i - (B.nv + B.no + B.nc);
     const int a = B.tri_v[t], b = B.tri_v[B.nt + t], c = B.tri_v[2 * (long long)B.nt + t];
     const long long nv = B.nv;
-    const float ax = x0v[a], ay = x0v[nv + a], az = x0v[2 * nv + a];
-    const float d1x = x0v[b] - ax, d1y = x0v[nv + b] - ay, d1z = x0v[2 * nv + b] - az;
-    const float d2x = x0v[c] - ax, d2y = x0v[nv + c] - ay, d2z = x0v[2 * nv + c] - az;
-    const float l1 = sqrtf(d1x * d1x + d1y * d1y + d1z * d1z + 1e-6f);
-    const float l2 = sqrtf(d2x * d2x + d2y * d2y + d2z * d2z + 1e-6f);
-    const float n1x = d1x / l1, n1y = d1y / l1, n1z = d1z / l1;
-    const float n2x = d2x / l2, n2y = d2y / l2, n2z = d2z / l2;
-    float nx = n1y * n2z - n1z * n2y, ny = n1z * n2x - n1x * n2z, nz = n1x * n2y - n1y * n2x;
-    const float l3 = sqrtf(nx * nx + ny * ny + nz * nz + 1e-6f);
-    nx /= l3; ny /= l3; nz /= l3;
-    // D0 = [d1 d2 n] (columns); inverse by the adjugate
-    const float m00 = d1x, m01 = d2x, m02 = nx, m10 = d1y, m11 = d2y, m12 = ny, m20 = d1z, m21 = d2z, m22 = nz;
-    const float c00 = m11 * m22 - m12 * m21, c01 = m02 * m21 - m01 * m22, c02 = m01 * m12 - m02 * m11;
-    const float c10 = m12 * m20 - m10 * m22, c11 = m00 * m22 - m02 * m20, c12 = m02 * m10 - m00 * m12;
-    const float c20 = m10 * m21 - m11 * m20, c21 = m01 * m20 - m00 * m21, c22 = m00 * m11 - m01 * m10;
-    const float det = m00 * c00 + m01 * c10 + m02 * c20;
-    const float id = 1.f / det;
-    const float inv[9] = {c00 * id, c01 * id, c02 * id, c10 * id, c11 * id, c12 * id, c20 * id, c21 * id, c22 * id};
+    const float pa[3] = {x0v[a], x0v[nv + a], x0v[2 * nv + a]};
+    const float pb[3] = {x0v[b], x0v[nv + b], x0v[2 * nv + b]};
+    const float pc[3] = {x0v[c], x0v[nv + c], x0v[2 * nv + c]};
+    float inv[9], nrm[3];
+    rest_frame(pa, pb, pc, inv, nrm);
     float* Di = const_cast<float*>(R.Di);
     float* n0 = const_cast<float*>(R.n0);
     for (int q = 0; q < 9; ++q) Di[q * (long long)B.nt + t] = inv[q];
     for (int q = 0; q < 12; ++q) S.t[q * (long long)B.nt + t] = 0.f;
-    n0[t] = nx;
-    n0[(long long)B.nt + t] = ny;
-    n0[2 * (long long)B.nt + t] = nz;
+    for (int q = 0; q < 3; ++q) n0[q * (long long)B.nt + t] = nrm[q];
   }
 }
 
@@ -161,7 +179,9 @@ __device__ __forceinline__ void lame(float E, float nu, float& mu, float& la) {
 // ============================================================== forward
 template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_tri_forward(BatchDev B, const float* __restrict__ params,
-                                                     const float* __restrict__ rest, const float* __restrict__ sin) {
+                                                     const float* __restrict__ rest, const float* __restrict__ sin,
+                                                     const int2* __restrict__ skip, const float* __restrict__ fdev) {
+  if (skip && skip->x >= 0) return;  // the grid of this substep is restored from the tape
   const Chunk ch = B.chunks[blockIdx.x];
   const InstDev& I = B.inst[ch.inst];
   const int tid = threadIdx.x;
@@ -187,6 +207,10 @@ __global__ void __launch_bounds__(256, MINB) k_tri_forward(BatchDev B, const flo
     load_tri_rest(B, R, S, t, dl3, n0, Di);
     M3<float> d, Fe;
     tri_F(g, dl3, n0, Di, d, Fe);
+    if (fdev) {  // stress from the F kept across a rest-frame reset (replay)
+#pragma unroll
+      for (int q = 0; q < 9; ++q) Fe.m[q] = __ldg(fdev + q * nt + t);
+    }
     Stress<float> sts;
     stress_forward<float>(Fe, mu, la, ks, kc, sts);
     const M3<float>& P = sts.P;
@@ -257,7 +281,9 @@ __device__ __forceinline__ bool operator_velocity(const BatchDev& B, const InstD
 }
 
 __global__ void __launch_bounds__(256) k_point_p2g(BatchDev B, const float* __restrict__ traj, int step, int window,
-                                                   const float* __restrict__ rest, const float* __restrict__ sin) {
+                                                   const float* __restrict__ rest, const float* __restrict__ sin,
+                                                   const int2* __restrict__ skip, float* __restrict__ fv_out) {
+  if (skip && skip->x >= 0) return;  // the grid of this substep is restored from the tape
   const Chunk ch = B.chunks[B.n_tri_chunks + blockIdx.x];
   const InstDev& I = B.inst[ch.inst];
   const int tid = threadIdx.x;
@@ -284,6 +310,10 @@ __global__ void __launch_bounds__(256) k_point_p2g(BatchDev B, const float* __re
         const int id = __ldg(B.inc_e + e);
 #pragma unroll
         for (int a = 0; a < 3; ++a) f[a] += B.force[a * e3 + id];
+      }
+      if (fv_out) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) fv_out[a * (long long)B.nv + p] = f[a];
       }
       // temp_v = v + (0, dt*scene_scaling*g, 0) (simulation.py:182)
       base_v[0] = m * __ldg(arr + 3 * n + p) + f[0];
@@ -338,8 +368,9 @@ __device__ __forceinline__ int kinematic_hit(const InstDev& I, const float* traj
 }
 
 __global__ void __launch_bounds__(256) k_grid(BatchDev B, const float* __restrict__ params,
-                                              const float* __restrict__ traj, int step, int mode) {
+                                              const float* __restrict__ traj, int step, int mode, TapeP T) {
   const int count = B.counters[0];
+  const int tape_at = T.meta ? T.meta[step].x : -1;
   const int per = blockDim.x >> 6, l = threadIdx.x & 63;
   for (int item = blockIdx.x * per + (threadIdx.x >> 6); item < count; item += gridDim.x * per) {
     const int blk = B.list_blk[item], inst = B.list_inst[item];
@@ -358,6 +389,14 @@ __global__ void __launch_bounds__(256) k_grid(BatchDev B, const float* __restric
       out[0] = __ldg(traj + o); out[1] = __ldg(traj + o + 1); out[2] = __ldg(traj + o + 2);
     }
     B.grid_v[n] = make_float4(out[0], out[1], out[2], 0.f);
+    if (tape_at >= 0) {
+      const long long slot = (long long)tape_at + item;
+      T.data[slot * 64 + l] = pm;
+      if (l == 0) {
+        T.blk[slot] = blk;
+        T.inst[slot] = inst;
+      }
+    }
     if (mode == GRID_FORWARD) {
       B.grid_pm[n] = make_float4(0.f, 0.f, 0.f, 0.f);
       if (l == 0) B.flags[blk] = 0u;
@@ -713,7 +752,8 @@ __device__ __forceinline__ float4 gadj(const BatchDev& B, const InstDev& I, int 
 // Reverse of k_point_p2g: gather dL/dp, dL/dm over the stencil.
 __global__ void __launch_bounds__(256) k_point_adj(BatchDev B, const float* __restrict__ traj, int step, int window,
                                                    const float* __restrict__ rest, const float* __restrict__ sin,
-                                                   float* __restrict__ ain, double* __restrict__ gtraj) {
+                                                   float* __restrict__ ain, double* __restrict__ gtraj,
+                                                   const int2* __restrict__ tmeta, const float* __restrict__ fv_in) {
   const Chunk ch = B.chunks[B.n_tri_chunks + blockIdx.x];
   if (threadIdx.x >= ch.count) return;
   const InstDev& I = B.inst[ch.inst];
@@ -736,12 +776,17 @@ __global__ void __launch_bounds__(256) k_point_adj(BatchDev B, const float* __re
   if (ch.kind == CHUNK_VERTEX) {
     m = I.m_v;
     float f[3] = {0.f, 0.f, 0.f};
-    const long long e3 = 3LL * B.nt;
-    const int e0 = __ldg(B.inc_ptr + p), e1 = __ldg(B.inc_ptr + p + 1);
-    for (int e = e0; e < e1; ++e) {
-      const int id = __ldg(B.inc_e + e);
+    if (fv_in && tmeta->x >= 0) {  // summed corner forces kept by the forward substep
 #pragma unroll
-      for (int a = 0; a < 3; ++a) f[a] += B.force[a * e3 + id];
+      for (int a = 0; a < 3; ++a) f[a] = __ldg(fv_in + a * (long long)B.nv + p);
+    } else {
+      const long long e3 = 3LL * B.nt;
+      const int e0 = __ldg(B.inc_ptr + p), e1 = __ldg(B.inc_ptr + p + 1);
+      for (int e = e0; e < e1; ++e) {
+        const int id = __ldg(B.inc_e + e);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) f[a] += B.force[a * e3 + id];
+      }
     }
     base_v[0] = m * __ldg(ai + 3 * n + p) + f[0];
     base_v[1] = m * (__ldg(ai + 4 * n + p) + I.gravity_dv) + f[1];
@@ -1082,10 +1127,92 @@ __global__ void k_chamfer_bwd(BatchDev B, const float* __restrict__ rest, const 
   }
 }
 
+// ============================================================== replay reset
+// reset_quadrature_particles (simulation_without_grad.py:471-485), triangle
+// part: the rest frame becomes [e1, e2, n] of the current vertices, d3 becomes
+// n (delta3 = 0), and the stored F is kept: F - I of the old frame goes to
+// fdev for the next substep's stress.  Runs before k_reset_vertex, which
+// moves the vertex rest positions to the current ones.
+__global__ void __launch_bounds__(256) k_reset_tri(BatchDev B, float* __restrict__ rest, float* __restrict__ state,
+                                                   float* __restrict__ fdev) {
+  StateP S = state_ptrs(state, B.nv, B.nt, B.no);
+  const RestP R = rest_ptrs(rest, B.nv, B.nt, B.no);
+  const long long nt = B.nt;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nt; t += (long long)gridDim.x * blockDim.x) {
+    TriGeom g;
+    load_tri(B, S, R, t, false, g);
+    float dl3[3], n0[3], Di[9];
+    load_tri_rest(B, R, S, t, dl3, n0, Di);
+    M3<float> d, Fe;
+    tri_F(g, dl3, n0, Di, d, Fe);
+    for (int q = 0; q < 9; ++q) fdev[q * nt + t] = Fe.m[q];
+    float p[3][3];
+    for (int c = 0; c < 3; ++c)
+      for (int a = 0; a < 3; ++a) p[c][a] = g.X0[c][a] + g.U[c][a];
+    float inv[9], nrm[3];
+    rest_frame(p[0], p[1], p[2], inv, nrm);
+    float* DiW = const_cast<float*>(R.Di);
+    float* n0W = const_cast<float*>(R.n0);
+    for (int q = 0; q < 9; ++q) DiW[q * nt + t] = inv[q];
+    for (int q = 0; q < 3; ++q) {
+      n0W[q * nt + t] = nrm[q];
+      S.t[(9 + q) * nt + t] = 0.f;
+    }
+  }
+}
+
+// Vertex part of the reset: rest position := current position, displacement 0.
+__global__ void __launch_bounds__(256) k_reset_vertex(BatchDev B, float* __restrict__ rest, float* __restrict__ state) {
+  StateP S = state_ptrs(state, B.nv, B.nt, B.no);
+  const RestP R = rest_ptrs(rest, B.nv, B.nt, B.no);
+  const long long nv = B.nv;
+  float* xv = const_cast<float*>(R.xv);
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < nv; p += (long long)gridDim.x * blockDim.x) {
+    for (int a = 0; a < 3; ++a) {
+      xv[a * nv + p] = xv[a * nv + p] + S.v[a * nv + p];
+      S.v[a * nv + p] = 0.f;
+    }
+  }
+}
+
+// ============================================================== grid tape
+// Reserve tape slots for the active blocks of substep `step` (one thread).
+__global__ void k_tape_reserve(BatchDev B, TapeP T, int step) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int count = B.counters[0];
+  const int top = *T.top;
+  if ((long long)top + count <= T.cap) {
+    T.meta[step] = make_int2(top, count);
+    *T.top = top + count;
+  } else {
+    T.meta[step] = make_int2(-1, count);
+  }
+}
+
+// Restore the (p, m) grid and the active-block list of substep `step`.
+__global__ void __launch_bounds__(256) k_tape_restore(BatchDev B, TapeP T, int step) {
+  const int2 m = T.meta[step];
+  if (m.x < 0) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) B.counters[0] = m.y;
+  const long long total = (long long)m.y * 64;
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
+    const long long item = g >> 6;
+    const int l = (int)(g & 63);
+    const long long slot = m.x + item;
+    const int blk = __ldg(T.blk + slot);
+    B.grid_pm[(long long)blk * 64 + l] = __ldg(T.data + slot * 64 + l);
+    if (l == 0) {
+      B.list_blk[item] = blk;
+      B.list_inst[item] = __ldg(T.inst + slot);
+      B.flags[blk] = 1u;
+    }
+  }
+}
+
 // ============================================================== launchers
 const char* const kKernelNames[KID_COUNT] = {
     "k_tri_forward", "k_point_p2g", "k_grid", "k_g2p", "k_g2p_adj", "k_grid_adj", "k_point_adj", "k_tri_adj",
-    "k_vertex_collect", "k_chamfer_fwd", "k_chamfer_loss", "k_chamfer_bwd", "k_init"};
+    "k_vertex_collect", "k_chamfer_fwd", "k_chamfer_loss", "k_chamfer_bwd", "k_init", "k_tape", "k_reset"};
 
 static inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 // Register-cap variants of the three register-heavy kernels: MINB resident
@@ -1108,37 +1235,67 @@ cudaError_t launch_init(const BatchDev& B, const LaunchCfg& L, const float* x0v,
 
 
 
+cudaError_t launch_reset(const BatchDev& B, const LaunchCfg& L, float* rest, float* state, float* fdev,
+                         cudaStream_t s) {
+  if (B.nt) {
+    const int grid = std::min(ceil_div(B.nt, 256), 148 * 16);
+    DCP_LAUNCH(KID_RESET, (k_reset_tri<<<grid, 256, 0, s>>>(B, rest, state, fdev)));
+  }
+  if (B.nv) {
+    const int grid = std::min(ceil_div(B.nv, 256), 148 * 16);
+    DCP_LAUNCH(KID_RESET, (k_reset_vertex<<<grid, 256, 0, s>>>(B, rest, state)));
+  }
+  return cudaGetLastError();
+}
+
+static TapeP no_tape() {
+  TapeP t;
+  t.top = nullptr; t.meta = nullptr; t.blk = nullptr; t.inst = nullptr; t.data = nullptr; t.fv = nullptr; t.cap = 0;
+  return t;
+}
+
 cudaError_t launch_forward(const BatchDev& B, const LaunchCfg& L, const float* params, const float* traj, const float* rest,
-                           int step, int window, const float* sin, float* sout, cudaStream_t s) {
+                           int step, int window, const float* sin, float* sout, cudaStream_t s, const TapeP* T,
+                           const float* fdev) {
+  const TapeP tp = T ? *T : no_tape();
   cudaMemsetAsync(B.counters, 0, sizeof(int), s);
   if (B.n_tri_chunks)
-    DCP_LAUNCH(KID_TRI_FORWARD, (DCP_MINB(k_tri_forward, L, 0)<<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin)));
+    DCP_LAUNCH(KID_TRI_FORWARD, (DCP_MINB(k_tri_forward, L, 0)<<<B.n_tri_chunks, L.block, 0, s>>>(
+                                    B, params, rest, sin, nullptr, fdev)));
   if (B.n_point_chunks)
-    DCP_LAUNCH(KID_POINT_P2G,
-               (k_point_p2g<<<B.n_point_chunks, L.block, 0, s>>>(B, traj, step, window, rest, sin)));
-  DCP_LAUNCH(KID_GRID, (k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_FORWARD)));
+    DCP_LAUNCH(KID_POINT_P2G, (k_point_p2g<<<B.n_point_chunks, L.block, 0, s>>>(
+                                  B, traj, step, window, rest, sin, nullptr,
+                                  T ? tp.fv + (long long)step * 3 * B.nv : nullptr)));
+  if (T) DCP_LAUNCH(KID_TAPE, (k_tape_reserve<<<1, 32, 0, s>>>(B, tp, step)));
+  DCP_LAUNCH(KID_GRID, (k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_FORWARD, tp)));
   DCP_LAUNCH(KID_G2P, (k_g2p<<<B.n_tri_chunks + B.n_point_chunks, L.block, 0, s>>>(B, params, rest, sin, sout)));
   return cudaGetLastError();
 }
 
 cudaError_t launch_backward(const BatchDev& B, const LaunchCfg& L, const float* params, const float* traj,
                             const float* rest, int step, int window, const float* sin, const float* aout, float* ain,
-                            double* gparams, double* gtraj, cudaStream_t s) {
+                            double* gparams, double* gtraj, cudaStream_t s, const TapeP* T) {
+  const TapeP none = no_tape();
+  const int2* meta = T ? T->meta + step : nullptr;
   cudaMemsetAsync(B.counters, 0, sizeof(int), s);
+  if (T) DCP_LAUNCH(KID_TAPE, (k_tape_restore<<<L.grid_ctas, 256, 0, s>>>(B, *T, step)));
   if (B.n_tri_chunks)
-    DCP_LAUNCH(KID_TRI_FORWARD, (DCP_MINB(k_tri_forward, L, 0)<<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin)));
+    DCP_LAUNCH(KID_TRI_FORWARD, (DCP_MINB(k_tri_forward, L, 0)<<<B.n_tri_chunks, L.block, 0, s>>>(
+                                    B, params, rest, sin, meta, nullptr)));
   if (B.n_point_chunks)
-    DCP_LAUNCH(KID_POINT_P2G,
-               (k_point_p2g<<<B.n_point_chunks, L.block, 0, s>>>(B, traj, step, window, rest, sin)));
-  DCP_LAUNCH(KID_GRID, (k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_RECOMPUTE)));
+    DCP_LAUNCH(KID_POINT_P2G, (k_point_p2g<<<B.n_point_chunks, L.block, 0, s>>>(B, traj, step, window, rest, sin,
+                                                                               meta, nullptr)));
+  DCP_LAUNCH(KID_GRID, (k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_RECOMPUTE, none)));
   DCP_LAUNCH(KID_G2P_ADJ, (DCP_MINB(k_g2p_adj, L, 1)<<<B.n_tri_chunks + B.n_point_chunks, L.block, 0, s>>>(
                               B, params, rest, sin, aout, ain, gparams)));
   DCP_LAUNCH(KID_GRID_ADJ, (k_grid_adj<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, gparams, gtraj)));
   if (B.n_point_chunks)
-    DCP_LAUNCH(KID_POINT_ADJ,
-               (k_point_adj<<<B.n_point_chunks, L.block, 0, s>>>(B, traj, step, window, rest, sin, ain, gtraj)));
+    DCP_LAUNCH(KID_POINT_ADJ, (k_point_adj<<<B.n_point_chunks, L.block, 0, s>>>(
+                                  B, traj, step, window, rest, sin, ain, gtraj, meta,
+                                  T ? T->fv + (long long)step * 3 * B.nv : nullptr)));
   if (B.n_tri_chunks)
-    DCP_LAUNCH(KID_TRI_ADJ, (DCP_MINB(k_tri_adj, L, 2)<<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin, ain, gparams)));
+    DCP_LAUNCH(KID_TRI_ADJ, (DCP_MINB(k_tri_adj, L, 2)<<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin, ain,
+                                                                                        gparams)));
   if (B.nv) DCP_LAUNCH(KID_VERTEX_COLLECT, (k_vertex_collect<<<ceil_div(B.nv, 256), 256, 0, s>>>(B, ain)));
   return cudaGetLastError();
 }

@@ -23,7 +23,7 @@ STATUS_OUT_OF_DOMAIN, STATUS_NONFINITE = 1, 2
 
 EXPORTED = (
     "dcp_plan", "dcp_create", "dcp_destroy", "dcp_sizes", "dcp_init_state", "dcp_substep_forward",
-    "dcp_substep_backward", "dcp_chamfer_forward", "dcp_chamfer_backward", "dcp_rollout_floats",
+    "dcp_substep_backward", "dcp_chamfer_forward", "dcp_chamfer_backward", "dcp_rollout_floats", "dcp_tape_bytes", "dcp_reset_quadrature", "dcp_replay",
     "dcp_rollout_state_offset", "dcp_rollout_forward", "dcp_rollout_backward", "dcp_read_status", "dcp_last_error",
     "dcp_launch_count", "dcp_profile", "dcp_profile_read", "dcp_kernel_count", "dcp_kernel_name",
     "dcp_chamfer_forward_static",
@@ -92,10 +92,14 @@ def lib():
     L.dcp_rollout_floats.restype = c_int64
     L.dcp_rollout_state_offset.argtypes = [c_void_p, c_int32, c_int32, c_int32]
     L.dcp_rollout_state_offset.restype = c_int64
+    L.dcp_reset_quadrature.argtypes = [c_void_p] * 5
+    L.dcp_replay.argtypes = [c_void_p] * 7 + [c_int32] * 4 + [c_void_p]
+    L.dcp_tape_bytes.argtypes = [c_void_p, c_int32, c_int64]
+    L.dcp_tape_bytes.restype = c_int64
     L.dcp_rollout_forward.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p,
-                                      c_int32, c_void_p]
+                                      c_void_p, c_int64, c_int32, c_void_p]
     L.dcp_rollout_backward.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_int32,
-                                       c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p]
+                                       c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p]
     L.dcp_read_status.argtypes = [c_void_p, P(c_int32), c_int32, c_void_p]
     L.dcp_last_error.restype = ctypes.c_char_p
     L.dcp_launch_count.argtypes = [c_void_p]

@@ -131,6 +131,25 @@ int dcp_init_state(DcpBatch* batch, const float* x0_vertex, const float* x0_oper
 int dcp_substep_forward(DcpBatch* batch, const float* params, const float* traj, const float* rest, int32_t step,
                         int32_t window, const float* state_in, float* state_out, void* stream);
 
+/* reset_quadrature_particles (simulation_without_grad.py:471-485) on every
+ * cloth: each triangle's rest frame becomes [e1, e2, n] of its current
+ * vertices (n: normalised cross product of the eps-normalised edges) and its
+ * d3 becomes n.  The reference keeps the stored deformation gradient F, so F - I
+ * of the old frame is written to fdev ([9][n_tri] floats) for the stress of
+ * the next substep (dcp_replay takes it).  The vertices' rest positions move
+ * to their current positions.  Rewrites `rest` and `state` in place. */
+int dcp_reset_quadrature(DcpBatch* batch, float* rest, float* state, float* fdev, void* stream);
+
+/* Forward-only replay (the loop of animation(), simulation_without_grad.py:
+ * 487-511): n_blocks times, block_steps substeps (step indices first_step,
+ * first_step + 1, ...; no window offset) followed by dcp_reset_quadrature.
+ * state: in/out; work: a second state buffer; fdev: [9][n_tri] floats.
+ * fdev_pending != 0: a reset came before first_step, so its substep takes the
+ * stress F from fdev.  After the call fdev is pending when n_blocks > 0. */
+int dcp_replay(DcpBatch* batch, const float* params, const float* traj, float* rest, float* state, float* work,
+               float* fdev, int32_t first_step, int32_t n_blocks, int32_t block_steps, int32_t fdev_pending,
+               void* stream);
+
 /* Reverse of one substep: backward(s, grad_update) of simulation.py:490-506.
  * Given state_in (state s) and adj_out (dL/d state s+1), writes adj_in
  * (dL/d state s) and accumulates grad_params / grad_traj. */
@@ -154,19 +173,33 @@ int64_t dcp_rollout_floats(const DcpBatch* batch, int32_t n_steps, int32_t ckpt_
  * rollout, or -1 when that state is not kept (it lies inside a segment). */
 int64_t dcp_rollout_state_offset(const DcpBatch* batch, int32_t n_steps, int32_t ckpt_every, int32_t step);
 
+/* Grid tape (optional; no counterpart in the reference, whose Taichi Tape
+ * re-runs P2G inside every adjoint substep): bytes of a tape that keeps, for
+ * each of n_steps substeps, the particle-to-grid result (momentum and mass of
+ * every active 4^3 node block, plus each vertex's summed corner force) of up to
+ * `blocks` active blocks in total.  With a tape, dcp_rollout_forward records
+ * and dcp_rollout_backward restores those grids instead of recomputing P2G;
+ * substeps that did not fit fall back to recomputing.  A tape belongs to one
+ * rollout: pass the same tape, tape_bytes and n_steps to both calls. */
+int64_t dcp_tape_bytes(const DcpBatch* batch, int32_t n_steps, int64_t blocks);
+
 /* The Tape-recorded loop of compute_grad (parameter_fitting_functions.py:25-28):
  * n_steps substeps from the state at offset 0 of `buf`, keeping checkpoints.
- * use_graph != 0 captures the launches once into a CUDA graph and replays it. */
+ * tape: NULL or a grid tape of tape_bytes (dcp_tape_bytes) that this call
+ * clears and fills.  use_graph != 0 captures the launches once into a CUDA
+ * graph and replays it. */
 int dcp_rollout_forward(DcpBatch* batch, const float* params, const float* traj, const float* rest, int32_t window,
-                        int32_t n_steps, int32_t ckpt_every, float* buf, int32_t use_graph, void* stream);
+                        int32_t n_steps, int32_t ckpt_every, float* buf, void* tape, int64_t tape_bytes,
+                        int32_t use_graph, void* stream);
 
 /* The Tape's reverse pass (parameter_fitting_functions.py:25-29 exit): adjoint
  * substeps loss_step-1 .. 0 with segment recompute.  adj_work: [2][state]; slot
  * 0 holds dL/d state(loss_step) on entry; on return dL/d state0 is in slot
- * (loss_step % 2). */
+ * (loss_step % 2).  tape: NULL or the tape the forward rollout filled. */
 int dcp_rollout_backward(DcpBatch* batch, const float* params, const float* traj, const float* rest, int32_t window,
                          int32_t n_steps, int32_t loss_step, int32_t ckpt_every, float* buf, float* adj_work,
-                         double* grad_params, double* grad_traj, int32_t use_graph, void* stream);
+                         double* grad_params, double* grad_traj, void* tape, int64_t tape_bytes, int32_t use_graph,
+                         void* stream);
 
 /* Kernel launch accounting.  dcp_launch_count: kernels issued on this batch
  * so far (graph replays add the kernels of the captured graph).

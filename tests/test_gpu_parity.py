@@ -65,6 +65,12 @@ def rel_err(got, ref):
 
 FIELDS = ("vx", "vv", "vC", "qC", "qd3", "ox", "ov", "oC", "cx", "cv", "cC")
 
+# Float atomics accumulate grid sums in a launch-dependent order, so runs that
+# differ in launch shape, particle order or what they recompute agree to
+# float32 rounding of those sums; gradients are compared at the parity bar
+# (1e-4 relative), losses tighter.
+ORDER_RTOL = 1e-4
+
 
 @pytest.mark.parametrize("window", [0, 1])
 def test_forward_substeps_match_oracle(window):
@@ -114,10 +120,11 @@ def test_reference_scene_loss_and_gradients(svd_grad):
     L = n - 2   # compute_loss(f) reads vertex_x[f - 1] after the loop (parameter_fitting_functions.py:7,27-29)
     b = _batch([sc], svd_grad=svd_grad)
     sim = BatchSim(b, n_steps=n, loss_step=L, ckpt_every=4)
-    params = b.params.clone().requires_grad_(True)
-    traj = b.traj.clone().requires_grad_(True)
-    loss = sim.loss(params, traj)
-    loss.sum().backward()
+    for _ in range(2):          # the second call restores the grids from the sized grid tape
+        params = b.params.clone().requires_grad_(True)
+        traj = b.traj.clone().requires_grad_(True)
+        loss = sim.loss(params, traj)
+        loss.sum().backward()
     p = oracle_params(sc, requires_grad=True)
     seq = torch.tensor(sc.keyframes, dtype=torch.float64, requires_grad=True)
     lo, p, seq, _, _ = oracle_loss(sc, n, L, params=p, seq=seq, svd_grad=svd_grad)
@@ -188,8 +195,53 @@ def test_checkpoint_interval_does_not_change_gradients(K):
         traj = b.traj.clone().requires_grad_(True)
         sim.loss(params, traj).sum().backward()
         res.append((params.grad.double().cpu().numpy(), traj.grad.double().cpu().numpy()))
-    np.testing.assert_allclose(res[0][0], res[1][0], rtol=1e-5, atol=1e-16)
-    np.testing.assert_allclose(res[0][1], res[1][1], rtol=1e-5, atol=1e-5 * np.abs(res[1][1]).max())
+    np.testing.assert_allclose(res[0][0], res[1][0], rtol=ORDER_RTOL, atol=1e-16)
+    np.testing.assert_allclose(res[0][1], res[1][1], rtol=ORDER_RTOL, atol=ORDER_RTOL * np.abs(res[1][1]).max())
+
+
+def _grads(sim, b, calls=1):
+    for _ in range(calls):
+        params = b.params.clone().requires_grad_(True)
+        traj = b.traj.clone().requires_grad_(True)
+        loss = sim.loss(params, traj)
+        loss.sum().backward()
+    return loss.detach().cpu().numpy(), params.grad.double().cpu().numpy(), traj.grad.double().cpu().numpy()
+
+
+@pytest.mark.parametrize("K", [1, 4])
+def test_grid_tape_matches_p2g_recompute(K):
+    """Restoring each substep's particle-to-grid result from the tape gives the
+    gradients of recomputing it, whether every substep fits or only some."""
+    from diffcp_b200.batch import BatchSim, ClothBatch
+    n = 16
+    sc = small_sheet(n_steps=n)
+    b0 = _batch([sc])
+    ref = _grads(BatchSim(b0, n_steps=n, ckpt_every=K, tape=None), b0)
+    b1 = _batch([sc])
+    sim = BatchSim(b1, n_steps=n, ckpt_every=K, tape="auto")
+    full = _grads(sim, b1, calls=2)                       # call 1 counts blocks, call 2 uses the tape
+    meta = ClothBatch.tape_blocks(sim._tape, n)
+    assert (meta[:, 0] >= 0).all() and (meta[:, 1] > 0).all()
+    half = int(meta[:, 1].sum() // 2)
+    b2 = _batch([sc])
+    sim2 = BatchSim(b2, n_steps=n, ckpt_every=K, tape=half)
+    part = _grads(sim2, b2)
+    meta2 = ClothBatch.tape_blocks(sim2._tape, n)
+    assert (meta2[:, 0] >= 0).any() and (meta2[:, 0] < 0).any()
+    for got in (full, part):
+        np.testing.assert_allclose(got[0], ref[0], rtol=1e-6)
+        np.testing.assert_allclose(got[1], ref[1], rtol=ORDER_RTOL, atol=1e-16)
+        np.testing.assert_allclose(got[2], ref[2], rtol=ORDER_RTOL, atol=ORDER_RTOL * np.abs(ref[2]).max())
+
+
+def test_grid_tape_too_small_for_its_fixed_part_is_rejected():
+    from diffcp_b200 import native
+    sc = small_sheet(n_steps=4)
+    b = _batch([sc])
+    buf = b.rollout_buffer(4, 1)
+    tape = torch.empty(64, dtype=torch.uint8, device=b.device)
+    with pytest.raises(RuntimeError, match="tape"):
+        b.rollout_forward(buf, 4, 1, tape=tape)
 
 
 def test_graph_replay_equals_eager():
@@ -207,7 +259,7 @@ def test_graph_replay_equals_eager():
         out.append((loss.detach().cpu().numpy(), params.grad.cpu().numpy()))
     for o in out[1:]:
         np.testing.assert_allclose(o[0], out[0][0], rtol=1e-6)
-        np.testing.assert_allclose(o[1], out[0][1], rtol=1e-5, atol=1e-16)
+        np.testing.assert_allclose(o[1], out[0][1], rtol=ORDER_RTOL, atol=1e-16)
 
 
 @pytest.mark.parametrize("chunk", [32, 64, 256])
@@ -217,8 +269,8 @@ def test_chunk_size_does_not_change_results(chunk):
     l1, g1, t1, _ = _sheet_grads(sc, n)
     l2, g2, t2, _ = _sheet_grads(sc, n, chunk=chunk)
     assert float(l1[0]) == pytest.approx(float(l2[0]), rel=1e-6)
-    np.testing.assert_allclose(g1, g2, rtol=1e-5, atol=1e-16)
-    np.testing.assert_allclose(t1, t2, rtol=1e-5, atol=1e-5 * np.abs(t1).max())
+    np.testing.assert_allclose(g1, g2, rtol=ORDER_RTOL, atol=1e-16)
+    np.testing.assert_allclose(t1, t2, rtol=ORDER_RTOL, atol=ORDER_RTOL * np.abs(t1).max())
 
 
 def test_unsorted_particle_order_matches_morton_order():
@@ -227,7 +279,7 @@ def test_unsorted_particle_order_matches_morton_order():
     l1, g1, t1, _ = _sheet_grads(sc, n)
     l2, g2, t2, _ = _sheet_grads(sc, n, reorder=False)
     assert float(l1[0]) == pytest.approx(float(l2[0]), rel=1e-6)
-    np.testing.assert_allclose(g1, g2, rtol=1e-5, atol=1e-16)
+    np.testing.assert_allclose(g1, g2, rtol=ORDER_RTOL, atol=1e-16)
 
 
 def test_chamfer_forward_argmin_and_backward():
