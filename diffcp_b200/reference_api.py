@@ -44,7 +44,8 @@ class _Grad:
         self._arr, self._idx = arr, idx
 
     def __getitem__(self, key):
-        return float(self._arr[self._idx])
+        # gradients accumulate in float64; reads see the float32 of the reference's f32 .grad field
+        return float(np.float32(self._arr[self._idx]))
 
     def __setitem__(self, key, value):
         self._arr[self._idx] = float(value)
@@ -62,6 +63,20 @@ class _ParamField:
 
     def __setitem__(self, key, value):
         _st.batch.params[0, self._col] = float(value)
+
+
+class _Scalar:
+    """Host-resident 0-D f32 field (the reference's learning_rate0..3,
+    taichi_variable_definition.py:10-14): stores float32, reads Python floats."""
+
+    def __init__(self, value=0.0):
+        self._v = np.float32(value)
+
+    def __getitem__(self, key):
+        return float(self._v)
+
+    def __setitem__(self, key, value):
+        self._v = np.float32(value)
 
 
 class _LossField:
@@ -221,12 +236,24 @@ def configure(src_dir: Optional[str] = None, seed: Optional[int] = 0, seed_cube:
         vertex_C=_HistoryField("vertex", "C"), operator_x=_HistoryField("operator", "x"),
         operator_v=_HistoryField("operator", "v"), cube_x=_HistoryField("cube", "x"),
         cube_v=_HistoryField("cube", "v"),
+        learning_rate0=_Scalar(), learning_rate1=_Scalar(), learning_rate2=_Scalar(), learning_rate3=_Scalar(),
     )
+    bounds = sc.meta.get("bounds", {})
+    for name in ("E", "nu", "contact_stiffness", "shearing_stiffness"):
+        if name in bounds:
+            g[name + "_lower_bound"], g[name + "_upper_bound"] = bounds[name]
+    for name, key in (("initial_garment_E", "E"), ("initial_garment_nu", "nu"),
+                      ("initial_contact_stiffness", "contact_stiffness"),
+                      ("initial_shearing_stiffness", "shearing_stiffness")):
+        g[name] = sc.params[key]
+    if src_dir is not None:
+        g["result_file_path"] = src_dir + sc.meta.get("result_dir", "/../result/") + "/fit_parameter.json"
     for name in ("garment_E", "garment_nu", "shearing_stiffness", "contact_stiffness", "loss", "grasp_tracking_seq",
                  "initial_vertex_x", "initial_operator_x", "initial_cube_x", "lagrangian_mesh_element",
                  "target_pos", "vertex_x", "vertex_v", "vertex_C", "operator_x", "operator_v", "cube_x",
                  "cube_v", "max_steps", "n_grad_updates", "target_pcd_array", "grasp_point_pos",
-                 "soft_body_model_vertices", "soft_body_mesh", "n_actions", "dt"):
+                 "soft_body_model_vertices", "soft_body_mesh", "n_actions", "dt", "learning_rate0",
+                 "learning_rate1", "learning_rate2", "learning_rate3"):
         if name not in __all__:
             __all__.append(name)
     _upload_targets(targets[0])

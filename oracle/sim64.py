@@ -29,6 +29,10 @@ kinematic sphere gripper on the grid (``KinematicGripper``); ``damping`` is the
 removed fraction of the symmetric part of the triangle ``C``, 0.95 in the
 reference (simulation.py:381-383).
 
+The forward-only replay of simulation_without_grad.py (same substep, frame
+index without window offset) adds ``OracleSim.reset_quadrature_particles``,
+which rebuilds the rest frames and leaves the stored ``F``, and ``replay``.
+
 Gradients: ``torch.autograd`` through the restatement.  ``svd_grad="exact"``
 differentiates the closed-form rotation factor of the 2x2 polar decomposition
 (the ``U V^T`` that the reference uses, simulation.py:235);
@@ -497,6 +501,45 @@ class OracleSim:
         new["qF"] = new_F
         new["qC"] = qC_new
         return new
+
+
+    # ---------------------------------------------------------------- replay
+    def reset_quadrature_particles(self, st: Dict[str, torch.Tensor]) -> Dict[str, torch.Tensor]:
+        """reset_quadrature_particles of simulation_without_grad.py:471-485:
+        triangle centroid, d = [e1, e2, n] of the current vertices (n from the
+        eps-normalised edges, norm(1e-6)) and a new rest-shape inverse; the
+        stored F (qF) is left as it is."""
+        vx = st["vx"]
+        a, b, c = vx[self.tris[:, 0]], vx[self.tris[:, 1]], vx[self.tris[:, 2]]
+        d1 = b - a
+        d2 = c - a
+        n1 = d1 / _norm_eps(d1, 1e-6)
+        n2 = d2 / _norm_eps(d2, 1e-6)
+        d3 = torch.cross(n1, n2, dim=-1)
+        d3 = d3 / _norm_eps(d3, 1e-6)
+        D = torch.stack((d1, d2, d3), dim=-1)
+        self.D0inv = torch.linalg.inv(D)
+        new = dict(st)
+        new["qx"] = (a + b + c) / 3
+        new["qd"] = D
+        return new
+
+
+def replay(sim: OracleSim, st, n_counts: int, block: int, params, seq=None, first_step: int = 0,
+           friction=None, damping=None, grip=None, on_count=None):
+    """The substep loop of animation() (simulation_without_grad.py:487-511):
+    ``n_counts`` times, ``block`` forward substeps (window 0) and a
+    reset_quadrature_particles; ``on_count(count, state)`` sees the state after
+    each reset.  Returns the final state."""
+    f = first_step
+    for count in range(n_counts):
+        for _ in range(block):
+            st = sim.substep(st, f, 0, params, seq=seq, friction=friction, damping=damping, grip=grip)
+            f += 1
+        st = sim.reset_quadrature_particles(st)
+        if on_count is not None:
+            on_count(count, st)
+    return st
 
 
 def compute_loss(vx: torch.Tensor, targets: torch.Tensor):

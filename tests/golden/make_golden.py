@@ -1,6 +1,7 @@
 """Generate the golden vectors in this folder by executing the reference's own
 source files (``src/initialization.py``, ``src/taichi_variable_definition.py``,
-``src/simulation.py``, ``src/parameter_fitting_functions.py`` of
+``src/simulation.py``, ``src/parameter_fitting_functions.py``,
+``src/simulation_without_grad.py`` of
 denzelzheng/diffcp) unmodified, under the NumPy stand-ins for ``taichi`` and
 ``open3d`` in ``ti_standin.py`` / ``o3d_standin.py``.
 
@@ -18,6 +19,12 @@ Outputs
                         respect to E, nu, contact/shearing stiffness and two
                         grasp-trajectory coordinates, reference kernels in
                         float64
+  ref_fitting.npz       the parameter-fitting step-size heuristic on random
+                        and edge inputs, and the epoch loop driven by the
+                        compute_grad stand-in of fit_fake.py
+  ref_replay_f32.npz    the forward-only replay of simulation_without_grad.py
+                        (substep blocks with reset_quadrature_particles) and
+                        the pose files animation() writes, float32
 
 Run:  python tests/golden/make_golden.py  [--ref PATH]   (needs the reference tree)
 """
@@ -243,24 +250,110 @@ def run_fd64(tree, out):
     np.savez_compressed(out, **rec)
 
 
+def run_fitting(tree, out):
+    """``single_parameter_fitting`` (parameter_fitting_functions.py:65-92) on
+    random and edge inputs, and ``parameters_learning`` (94-205) driven by the
+    deterministic compute_grad stand-in of fit_fake.py."""
+    import contextlib
+    import io
+    m = import_reference(tree)
+    import fit_fake
+    rng = np.random.default_rng(99)
+    rows_in, rows_out = [], []
+    for k in range(600):
+        name = fit_fake.NAMES[k % 4]
+        lo, hi = fit_fake.BOUNDS[name]
+        p = float(rng.uniform(lo, hi))
+        if k % 50 == 7:
+            g = 0.0
+        elif k % 50 == 13:
+            g = float("nan")
+        else:
+            g = float((1 if rng.random() < 0.5 else -1) * 10.0 ** rng.uniform(-8, 8))
+        lr = float(10.0 ** rng.uniform(-6, 3))
+        epochs = int(rng.integers(2, 40))
+        idx = 0 if k % 3 == 0 else int(rng.integers(0, epochs))
+        res = m.single_parameter_fitting(p, g, 0, lo, hi, lr, epochs, idx)
+        rows_in.append([p, g, lo, hi, lr, epochs, idx])
+        rows_out.append([float(res[0]), float(res[1])])
+    rec = {"spf_in": np.array(rows_in), "spf_out": np.array(rows_out)}
+    for (name, init, tgt, w, epochs, nan_g, nan_l, flags) in fit_fake.scenarios():
+        calls = fit_fake.install(m, init, tgt, w, nan_g, nan_l)
+        with contextlib.redirect_stdout(io.StringIO()):
+            m.parameters_learning(flags[0], flags[1], epochs)
+        rec["calls_" + name] = np.array(calls)
+        rec["final_" + name] = np.array([getattr(m, fit_fake.FIELD[n])[None] for n in fit_fake.NAMES])
+        rec["loss_" + name] = np.array(m.loss[None])
+    np.savez_compressed(out, **rec)
+
+
+def run_replay(tree, out):
+    """The forward-only replay of ``src/simulation_without_grad.py``: six
+    blocks of int(IFS/dt) substeps, each followed by
+    reset_quadrature_particles, recording the state after every reset; then
+    ``animation()`` itself with the open3d stand-in recording which pose files
+    it writes and their vertices."""
+    sys.path.insert(0, HERE)
+    import ti_standin
+    import o3d_standin
+    import types
+    sys.modules["taichi"] = ti_standin
+    sys.modules["taichi_glsl"] = types.ModuleType("taichi_glsl")
+    sys.modules["open3d"] = o3d_standin
+    random.seed(SEED_OP)
+    np.random.seed(SEED_CUBE)
+    sys.path.insert(0, tree)
+    import src.simulation_without_grad as m   # noqa: E402
+    m.garment_E[None] = PARAMS["E"]
+    m.garment_nu[None] = PARAMS["nu"]
+    m.contact_stiffness[None] = PARAMS["contact_stiffness"]
+    m.shearing_stiffness[None] = PARAMS["shearing_stiffness"]
+    m.initialize_objects()
+    block = int(0.001 / m.dt)
+    rec = {"block": np.array(block)}
+    f = 0
+    for count in range(6):
+        for _ in range(block):
+            m.forward(f)
+            f += 1
+        m.reset_quadrature_particles()
+        for k in ("vertex_x", "vertex_v", "quadrature_d", "quadrature_F", "initial_quadrature_d_inv", "operator_x"):
+            rec["c%d_%s" % (count, k)] = getattr(m, k).to_numpy()
+    writes = []
+    o3d_standin.io.write_triangle_mesh = lambda path, mesh, **kw: writes.append(
+        (int(os.path.basename(path)[:-4]), np.asarray(mesh.vertices, dtype=np.float64).copy())) or True
+    m.initialize_objects()
+    anim = m.operator_update_interval * (m.n_actions - 1)
+    m.animation(anim)
+    rec["animation_time"] = np.array(anim)
+    rec["n_pose_estimation_output"] = np.array(m.n_pose_estimation_output)
+    rec["pose_index"] = np.array([w[0] for w in writes])
+    rec["pose_vertices"] = np.stack([w[1] for w in writes]) if writes else np.zeros((0, 0, 3))
+    np.savez_compressed(out, **rec)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--mode", default="all", choices=["all", "forward32", "svd", "fd64"])
+    ap.add_argument("--mode", default="all", choices=["all", "forward32", "svd", "fd64", "fitting", "replay"])
     ap.add_argument("--tree")
+    ap.add_argument("--only", nargs="*", help="with --mode all: the modes to regenerate")
     a = ap.parse_args()
     if a.mode == "all":
         tree = build_tree(a.ref)
         try:
-            for mode in ("forward32", "svd", "fd64"):
+            for mode in a.only or ("forward32", "svd", "fd64", "fitting", "replay"):
                 t0 = time.time()
                 subprocess.run([sys.executable, __file__, "--mode", mode, "--tree", tree], check=True)
                 print("%s done in %.1f s" % (mode, time.time() - t0))
         finally:
             shutil.rmtree(tree, ignore_errors=True)
         return
-    out = {"forward32": "ref_forward_f32.npz", "svd": "ref_svd_backward.npz", "fd64": "ref_fd_f64.npz"}[a.mode]
-    {"forward32": run_forward32, "svd": run_svd, "fd64": run_fd64}[a.mode](a.tree, os.path.join(HERE, out))
+    out = {"forward32": "ref_forward_f32.npz", "svd": "ref_svd_backward.npz", "fd64": "ref_fd_f64.npz",
+           "fitting": "ref_fitting.npz", "replay": "ref_replay_f32.npz"}[a.mode]
+    {"forward32": run_forward32, "svd": run_svd, "fd64": run_fd64, "fitting": run_fitting,
+     "replay": run_replay}[a.mode](
+        a.tree, os.path.join(HERE, out))
 
 
 if __name__ == "__main__":
