@@ -80,16 +80,49 @@ def _read_ascii(tok, elements):
     return verts, tris
 
 
-def write_ply(path, vertices, triangles):
+def vertex_normals(vertices, triangles):
+    """Unit vertex normals: the sum of the adjacent triangles' cross-product
+    (area-weighted) normals, normalised."""
+    v = np.asarray(vertices, dtype=np.float64)
+    t = np.asarray(triangles, dtype=np.int64)
+    fn = np.cross(v[t[:, 1]] - v[t[:, 0]], v[t[:, 2]] - v[t[:, 0]])
+    n = np.zeros_like(v)
+    for k in range(3):
+        np.add.at(n, t[:, k], fn)
+    ln = np.linalg.norm(n, axis=1, keepdims=True)
+    return np.divide(n, ln, out=np.zeros_like(n), where=ln > 0)
+
+
+def write_ply(path, vertices, triangles, normals=None, colors=None):
+    """Binary little-endian PLY: double x, y, z [+ double nx, ny, nz]
+    [+ uchar red, green, blue] per vertex, ``list uchar uint`` faces -- the
+    layout Open3D's write_triangle_mesh produces for the reference's pose
+    meshes (simulation_without_grad.py:512-520).  ``colors``: (3,) or (N, 3)
+    in [0, 1]."""
     v = np.asarray(vertices, dtype="<f8")
     t = np.asarray(triangles, dtype="<u4")
-    head = ("ply\nformat binary_little_endian 1.0\nelement vertex %d\nproperty double x\nproperty double y\n"
-            "property double z\nelement face %d\nproperty list uchar uint vertex_indices\nend_header\n"
-            % (len(v), len(t)))
+    fields = [("x", "<f8"), ("y", "<f8"), ("z", "<f8")]
+    props = "property double x\nproperty double y\nproperty double z\n"
+    if normals is not None:
+        fields += [("nx", "<f8"), ("ny", "<f8"), ("nz", "<f8")]
+        props += "property double nx\nproperty double ny\nproperty double nz\n"
+    if colors is not None:
+        fields += [("red", "u1"), ("green", "u1"), ("blue", "u1")]
+        props += "property uchar red\nproperty uchar green\nproperty uchar blue\n"
+    rows = np.zeros(len(v), dtype=fields)
+    rows["x"], rows["y"], rows["z"] = v[:, 0], v[:, 1], v[:, 2]
+    if normals is not None:
+        nrm = np.asarray(normals, dtype=np.float64)
+        rows["nx"], rows["ny"], rows["nz"] = nrm[:, 0], nrm[:, 1], nrm[:, 2]
+    if colors is not None:
+        col = np.broadcast_to(np.clip(np.rint(np.asarray(colors, dtype=np.float64) * 255.0), 0, 255), (len(v), 3))
+        rows["red"], rows["green"], rows["blue"] = col[:, 0], col[:, 1], col[:, 2]
+    head = ("ply\nformat binary_little_endian 1.0\nelement vertex %d\n%selement face %d\n"
+            "property list uchar uint vertex_indices\nend_header\n" % (len(v), props, len(t)))
     rec = np.zeros(len(t), dtype=[("n", "u1"), ("idx", "<u4", (3,))])
     rec["n"] = 3
     rec["idx"] = t
     with open(path, "wb") as fh:
         fh.write(head.encode("ascii"))
-        fh.write(v.tobytes())
+        fh.write(rows.tobytes())
         fh.write(rec.tobytes())
