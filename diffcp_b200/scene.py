@@ -141,7 +141,7 @@ def reference_scene(args: dict, mesh_vertices, mesh_triangles, grasp_seq, target
                 "friction": 0.0, "damping": REFERENCE_DAMPING},
         meta={"dt": dt, "max_steps": int(gui / dt) + 1, "targets_by_window": target, "area": area,
               "garment_mass": garment_mass, "n_actions": n_actions, "operator_model": op_model,
-              "grad_update_interval": gui, "scene_scaling": s,
+              "grad_update_interval": gui, "scene_scaling": s, "shift": shift,
               "bounds": {k: (gp["constitutive_parameter_lower_bounds"][k], gp["constitutive_parameter_upper_bounds"][k])
                          for k in ("E", "nu", "contact_stiffness", "shearing_stiffness")},
               "result_dir": args.get("result_dir", "/../result/")},
