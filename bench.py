@@ -39,7 +39,6 @@ sys.path.insert(0, ROOT)
 
 METRIC = "fwd+bwd particle-steps/s"
 UNIT = "particle-steps/s"
-SPACING = 0.2 / 31
 # Algorithmic bytes per particle of one launch (float32 state, grid traffic
 # excluded), for each kernel of the substep and its adjoint; see DESIGN.md.
 KERNEL_BYTES = {
@@ -58,31 +57,17 @@ STEP_BYTES = {"vertex": 420, "tri": 1068}
 
 
 def workload(name, seed):
-    from diffcp_b200 import scene
+    from diffcp_b200 import configs
     if name == "sweep":
-        rng = np.random.default_rng(seed)
-        scenes = []
-        for i in range(256):
-            n = int(rng.integers(16, 97))
-            E = float(10 ** rng.uniform(3, 5))
-            nu = float(rng.uniform(0.1, 0.45))
-            fr = float(rng.uniform(0.1, 0.6))
-            scenes.append(scene.sheet_scene(n=n, side=(n - 1) * SPACING, height=0.3, n_grid=64, dt=1e-4,
-                                            n_steps=300, E=E, nu=nu, friction=fr, seed=seed * 1000 + i,
-                                            n_targets=2048))
-        return scenes, dict(dt=1e-4, n_steps=300, ckpt_every=1,
-                            desc="batched parameter sweep: 256 cloths, side U{16..96} vertices, 64^3 grid each, "
-                                 "dt 1e-4, 300 substeps, Chamfer to 2048 targets each")
+        return configs.parameter_sweep(seed)
     if name == "single":
-        return [scene.sheet_scene(n=128, side=0.4, height=0.3, n_grid=128, dt=1e-4, n_steps=1000, seed=seed,
-                                  n_targets=2048)], dict(
-            dt=1e-4, n_steps=1000, ckpt_every=50,
-            desc="single cloth 128x128 vertices, 0.4 m, 128^3 grid, dt 1e-4, 1000 substeps, checkpoints every 50")
+        return configs.large_sheet(seed)
     if name == "small":
-        return [scene.sheet_scene(n=32, side=0.2, height=0.3, n_grid=64, dt=2e-4, n_steps=200, seed=seed,
-                                  n_targets=2048)], dict(
-            dt=2e-4, n_steps=200, ckpt_every=1,
-            desc="single cloth 32x32 vertices, 0.2 m, 64^3 grid, dt 2e-4, 200 substeps")
+        return configs.single_sheet(seed)
+    if name == "traj":
+        return configs.trajectory_batch(seed)
+    if name == "stress":
+        return configs.stress_sheet(seed)
     raise ValueError(name)
 
 
@@ -208,9 +193,13 @@ def profile_substeps(args):
     """A few eager substeps and adjoint substeps of the workload on a handful
     of state buffers (a few GB on the device), for kernel profilers."""
     import torch
+    from diffcp_b200 import autotune
     from diffcp_b200.batch import ClothBatch
     scenes, info = workload(args.workload, 0)
-    b = ClothBatch(scenes, dt=info["dt"])
+    cache = args.tune_cache or autotune.CACHE
+    launch = (autotune.cached(scenes, info["dt"], cache=cache) if os.path.exists(cache) else None) or autotune.DEFAULT
+    b = ClothBatch(scenes, dt=info["dt"], chunk=launch["chunk"], scatter_mode=launch["scatter_mode"],
+                   min_blocks=launch["min_blocks"])
     n = args.profile_substeps
     states = [b.init_state()]
     for f in range(n):
@@ -233,7 +222,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "single", "small"])
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "single", "small", "traj", "stress"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
@@ -431,7 +420,8 @@ def main():
                    "l2": "inputs larger than L2 (state snapshot %.0f MB, rollout buffer %.1f GB)"
                          % (batch.S * 4 / 1e6, sim._buf.numel() * 4 / 1e9),
                    "parallelism": "independent instances per rank" if world > 1 else "one GPU",
-                   "launch": launch, "grid_tape": tape_info},
+                   "launch": launch, "grid_tape": tape_info,
+                   "peak_device_bytes": int(torch.cuda.max_memory_allocated(dev))},
         "roofline": roof,
         "step_roofline": {"achieved": step_alg / (ms_max / 1e3) / 1e9, "unit": "GB/s", "peak": peak,
                           "frac": step_alg / (ms_max / 1e3) / 1e9 / peak,

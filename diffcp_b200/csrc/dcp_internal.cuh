@@ -130,10 +130,31 @@ __device__ __forceinline__ long long node_index(const InstDev& I, int i, int j, 
   return I.node_off + (long long)blk * 64 + within;
 }
 
+// Per-axis parts of the block-major index of a stencil's 27 nodes: node
+// (base + (oi, oj, ok)) of instance I sits at I.node_off + ax[oi] + ay[oj] +
+// az[ok] (the same value as node_index, formed with two adds per node).
+struct NodeOffsets {
+  int ax[3], ay[3], az[3];
+};
+__device__ __forceinline__ NodeOffsets node_offsets(const InstDev& I, const int base[3]) {
+  NodeOffsets o;
+  const int sy = I.nb * 64, sx = I.nb * sy;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const int i = base[0] + q, j = base[1] + q, k = base[2] + q;
+    o.ax[q] = (i >> 2) * sx + ((i & 3) << 4);
+    o.ay[q] = (j >> 2) * sy + ((j & 3) << 2);
+    o.az[q] = ((k >> 2) << 6) + (k & 3);
+  }
+  return o;
+}
+
 // Quadratic B-spline stencil of one particle (simulation.py:140-142): base node
 // = trunc(x/dx - 0.5) per axis, fractional offset fx, 1-D weights and slopes.
 // Out-of-domain bases are clamped so every access stays inside the instance's
-// grid, and the instance is flagged.
+// grid, and the instance is flagged.  The cell coordinate is formed with
+// explicitly rounded operations (no multiply-add contraction), so every kernel
+// that builds the stencil of the same particle gets the same base cell.
 struct Sten {
   int base[3];
   float fx[3];
@@ -144,8 +165,8 @@ __device__ __forceinline__ void make_stencil(const float p[3], const InstDev& I,
   bool bad = false;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const float sx = p[a] * I.inv_dx;
-    const float t = sx - 0.5f;
+    const float sx = __fmul_rn(p[a], I.inv_dx);
+    const float t = __fsub_rn(sx, 0.5f);
     int b = (int)t;
     if (!(t >= 0.f) || b > I.G - 3) {
       bad = true;
@@ -153,7 +174,7 @@ __device__ __forceinline__ void make_stencil(const float p[3], const InstDev& I,
       if (!(t == t)) b = 0;
     }
     s.base[a] = b;
-    s.fx[a] = sx - (float)b;
+    s.fx[a] = __fsub_rn(sx, (float)b);
     bspline(s.fx[a], s.w[a], s.dw[a]);
   }
   if (bad) atomicOr(status + inst, STATUS_OUT_OF_DOMAIN);
@@ -185,7 +206,7 @@ template <bool MARK, class F>
 __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I, int inst, const int base[3],
                                              bool valid, F&& contrib) {
   const unsigned FULL = 0xffffffffu;
-  float4* grid = MARK ? B.grid_pm : B.grid_adj;
+  float4* grid = (MARK ? B.grid_pm : B.grid_adj) + I.node_off;
   if (B.scatter_mode == 1) {  // per-lane atomics: no shuffles, more L2 traffic
     if (!valid) return;
     if (MARK) {
@@ -202,6 +223,7 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
             mark_block(node_index(I, i, j, k), B.flags, B.list_blk, B.list_inst, B.counters, inst);
           }
     }
+    const NodeOffsets no = node_offsets(I, base);
 #pragma unroll
     for (int oi = 0; oi < 3; ++oi)
 #pragma unroll
@@ -210,7 +232,7 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
         for (int ok = 0; ok < 3; ++ok) {
           const float4 v = contrib(oi, oj, ok);
           if (v.x != 0.f || v.y != 0.f || v.z != 0.f || v.w != 0.f)
-            atomicAdd(grid + node_index(I, base[0] + oi, base[1] + oj, base[2] + ok), v);
+            atomicAdd(grid + (no.ax[oi] + no.ay[oj] + no.az[ok]), v);
         }
     return;
   }
@@ -245,6 +267,7 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
           mark_block(node_index(I, i, j, k), B.flags, B.list_blk, B.list_inst, B.counters, inst);
         }
   }
+  const NodeOffsets no = node_offsets(I, base);
 #pragma unroll
   for (int oi = 0; oi < 3; ++oi)
 #pragma unroll
@@ -266,7 +289,7 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
           }
         }
         if (head && valid && (v.x != 0.f || v.y != 0.f || v.z != 0.f || v.w != 0.f))
-          atomicAdd(grid + node_index(I, base[0] + oi, base[1] + oj, base[2] + ok), v);
+          atomicAdd(grid + (no.ax[oi] + no.ay[oj] + no.az[ok]), v);
       }
 }
 

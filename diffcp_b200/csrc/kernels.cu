@@ -406,28 +406,33 @@ __global__ void __launch_bounds__(256) k_grid(BatchDev B, const float* __restric
   }
 }
 
-__device__ __forceinline__ float3 gv(const BatchDev& B, const InstDev& I, int i, int j, int k) {
-  const float4 v = __ldg(B.grid_v + node_index(I, i, j, k));
+__device__ __forceinline__ float3 gv_at(const float4* g, const NodeOffsets& o, int oi, int oj, int ok) {
+  const float4 v = __ldg(g + (o.ax[oi] + o.ay[oj] + o.az[ok]));
   return make_float3(v.x, v.y, v.z);
 }
 
+// TRI: launched over the triangle chunks; otherwise over the point chunks
+// (vertex, operator, cube), which follow the triangle chunks in the table.
+template <bool TRI>
 __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict__ params,
                                              const float* __restrict__ rest, const float* __restrict__ sin,
                                              float* __restrict__ sout) {
-  const Chunk ch = B.chunks[blockIdx.x];
+  const Chunk ch = B.chunks[(TRI ? 0 : B.n_tri_chunks) + blockIdx.x];
   if (threadIdx.x >= ch.count) return;
   const InstDev& I = B.inst[ch.inst];
   StateP Si = state_ptrs(const_cast<float*>(sin), B.nv, B.nt, B.no);
   StateP So = state_ptrs(sout, B.nv, B.nt, B.no);
   const RestP R = rest_ptrs(rest, B.nv, B.nt, B.no);
   const float dt = B.dt, inv_dx = I.inv_dx;
-  if (ch.kind == CHUNK_TRI) {
+  if (TRI) {
     const long long t = ch.start + threadIdx.x, nt = B.nt;
     TriGeom g;
     load_tri(B, Si, R, t, false, g);
     Sten st;
     make_stencil(g.xc, I, st, B.status, ch.inst);
     float Ct[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const float4* gnb = B.grid_v + I.node_off;
+    const NodeOffsets nofs = node_offsets(I, st.base);
 #pragma unroll
     for (int oi = 0; oi < 3; ++oi)
 #pragma unroll
@@ -435,7 +440,7 @@ __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict
 #pragma unroll
         for (int ok = 0; ok < 3; ++ok) {
           const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
-          const float3 gn = gv(B, I, st.base[0] + oi, st.base[1] + oj, st.base[2] + ok);
+          const float3 gn = gv_at(gnb, nofs, oi, oj, ok);
           const float dp[3] = {(float)oi - st.fx[0], (float)oj - st.fx[1], (float)ok - st.fx[2]};
           const float s = 4.f * W * inv_dx;
           const float ga[3] = {gn.x, gn.y, gn.z};
@@ -496,6 +501,8 @@ __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict
   Sten st;
   make_stencil(X, I, st, B.status, ch.inst);
   float v[3] = {0.f, 0.f, 0.f}, C[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  const float4* gnb = B.grid_v + I.node_off;
+  const NodeOffsets nofs = node_offsets(I, st.base);
 #pragma unroll
   for (int oi = 0; oi < 3; ++oi)
 #pragma unroll
@@ -503,7 +510,7 @@ __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict
 #pragma unroll
       for (int ok = 0; ok < 3; ++ok) {
         const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
-        const float3 gn = gv(B, I, st.base[0] + oi, st.base[1] + oj, st.base[2] + ok);
+        const float3 gn = gv_at(gnb, nofs, oi, oj, ok);
         const float dp[3] = {(float)oi - st.fx[0], (float)oj - st.fx[1], (float)ok - st.fx[2]};
         const float ga[3] = {gn.x, gn.y, gn.z};
         const float s = 4.f * W * inv_dx;
@@ -571,12 +578,14 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
     if (tri) {
       const long long nt = B.nt;
       float Ct[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      const float4* gnb = B.grid_v + I.node_off;
+      const NodeOffsets nofs = node_offsets(I, st.base);
 #pragma unroll
       for (int q = 0; q < 27; ++q) {
         const int oi = q / 9, oj = (q / 3) % 3, ok = q % 3;
         const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
         const float dp[3] = {(float)oi - st.fx[0], (float)oj - st.fx[1], (float)ok - st.fx[2]};
-        const float3 gn = gv(B, I, st.base[0] + oi, st.base[1] + oj, st.base[2] + ok);
+        const float3 gn = gv_at(gnb, nofs, oi, oj, ok);
         const float ga[3] = {gn.x, gn.y, gn.z};
         const float s = 4.f * W * inv_dx;
 #pragma unroll
@@ -660,6 +669,8 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
     // position adjoint of the gather (second pass over the stencil)
     float px[3] = {0.f, 0.f, 0.f};
     const float c4 = 4.f * inv_dx;
+    const float4* gnb = B.grid_v + I.node_off;
+    const NodeOffsets nofs = node_offsets(I, st.base);
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
       const int oi = q / 9, oj = (q / 3) % 3, ok = q % 3;
@@ -667,7 +678,7 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
       const float W = w0 * w1 * w2;
       const float gW[3] = {st.dw[0][oi] * w1 * w2 * inv_dx, w0 * st.dw[1][oj] * w2 * inv_dx, w0 * w1 * st.dw[2][ok] * inv_dx};
       const float dp[3] = {(float)oi - st.fx[0], (float)oj - st.fx[1], (float)ok - st.fx[2]};
-      const float3 gn = gv(B, I, st.base[0] + oi, st.base[1] + oj, st.base[2] + ok);
+      const float3 gn = gv_at(gnb, nofs, oi, oj, ok);
       const float ga[3] = {gn.x, gn.y, gn.z};
       float s1 = bV[0] * ga[0] + bV[1] * ga[1] + bV[2] * ga[2];
 #pragma unroll
@@ -745,10 +756,6 @@ __global__ void __launch_bounds__(256) k_grid_adj(BatchDev B, const float* __res
   }
 }
 
-__device__ __forceinline__ float4 gadj(const BatchDev& B, const InstDev& I, int i, int j, int k) {
-  return __ldg(B.grid_adj + node_index(I, i, j, k));
-}
-
 // Reverse of k_point_p2g: gather dL/dp, dL/dm over the stencil.
 __global__ void __launch_bounds__(256) k_point_adj(BatchDev B, const float* __restrict__ traj, int step, int window,
                                                    const float* __restrict__ rest, const float* __restrict__ sin,
@@ -806,6 +813,8 @@ __global__ void __launch_bounds__(256) k_point_adj(BatchDev B, const float* __re
   float sp[3] = {0.f, 0.f, 0.f};     // sum W bp
   float spd[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // sum W bp (x) dpos
   float px[3] = {0.f, 0.f, 0.f};
+  const float4* gnb = B.grid_adj + I.node_off;
+  const NodeOffsets nofs = node_offsets(I, st.base);
 #pragma unroll
   for (int q = 0; q < 27; ++q) {
     const int oi = q / 9, oj = (q / 3) % 3, ok = q % 3;
@@ -813,7 +822,7 @@ __global__ void __launch_bounds__(256) k_point_adj(BatchDev B, const float* __re
     const float W = w0 * w1 * w2;
     const float gW[3] = {st.dw[0][oi] * w1 * w2 * inv_dx, w0 * st.dw[1][oj] * w2 * inv_dx, w0 * w1 * st.dw[2][ok] * inv_dx};
     const float dp[3] = {((float)oi - st.fx[0]) * dx, ((float)oj - st.fx[1]) * dx, ((float)ok - st.fx[2]) * dx};
-    const float4 g = gadj(B, I, st.base[0] + oi, st.base[1] + oj, st.base[2] + ok);
+    const float4 g = __ldg(gnb + (nofs.ax[oi] + nofs.ay[oj] + nofs.az[ok]));
     const float bp[3] = {g.x, g.y, g.z};
     float s = g.w * m;
     float ctb[3] = {0.f, 0.f, 0.f};
@@ -899,6 +908,8 @@ __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* 
     float bP3[3] = {0.f, 0.f, 0.f}, bd3[3] = {0.f, 0.f, 0.f}, bx[3] = {0.f, 0.f, 0.f};
     const float mv[3] = {m * g.vc[0], m * g.vc[1], m * g.vc[2]};
     const float i2 = inv_dx * inv_dx;
+    const float4* gnb = B.grid_adj + I.node_off;
+    const NodeOffsets nofs = node_offsets(I, st.base);
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
       const int oi = q / 9, oj = (q / 3) % 3, ok = q % 3;
@@ -911,7 +922,7 @@ __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* 
                           e0 * e1 * w2 * i2, w0 * dd1 * w2 * i2, w0 * e1 * e2 * i2,
                           e0 * w1 * e2 * i2, w0 * e1 * e2 * i2, w0 * w1 * dd2 * i2};
       const float dp[3] = {((float)oi - st.fx[0]) * dx, ((float)oj - st.fx[1]) * dx, ((float)ok - st.fx[2]) * dx};
-      const float4 ga = gadj(B, I, st.base[0] + oi, st.base[1] + oj, st.base[2] + ok);
+      const float4 ga = __ldg(gnb + (nofs.ax[oi] + nofs.ay[oj] + nofs.az[ok]));
       const float bp[3] = {ga.x, ga.y, ga.z};
       const float gdot = gW[0] * d3[0] + gW[1] * d3[1] + gW[2] * d3[2];
       const float sP = bp[0] * P3[0] + bp[1] * P3[1] + bp[2] * P3[2];
@@ -1268,7 +1279,10 @@ cudaError_t launch_forward(const BatchDev& B, const LaunchCfg& L, const float* p
                                   T ? tp.fv + (long long)step * 3 * B.nv : nullptr)));
   if (T) DCP_LAUNCH(KID_TAPE, (k_tape_reserve<<<1, 32, 0, s>>>(B, tp, step)));
   DCP_LAUNCH(KID_GRID, (k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_FORWARD, tp)));
-  DCP_LAUNCH(KID_G2P, (k_g2p<<<B.n_tri_chunks + B.n_point_chunks, L.block, 0, s>>>(B, params, rest, sin, sout)));
+  if (B.n_tri_chunks)
+    DCP_LAUNCH(KID_G2P, (k_g2p<true><<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin, sout)));
+  if (B.n_point_chunks)
+    DCP_LAUNCH(KID_G2P, (k_g2p<false><<<B.n_point_chunks, L.block, 0, s>>>(B, params, rest, sin, sout)));
   return cudaGetLastError();
 }
 

@@ -111,13 +111,14 @@ def stencil(x: torch.Tensor, inv_dx: float):
     base = torch.trunc(s).to(torch.long)
     fx = x * inv_dx - base.to(x.dtype)
     w = torch.stack((0.5 * (1.5 - fx) ** 2, 0.75 - (fx - 1.0) ** 2, 0.5 * (fx - 0.5) ** 2), dim=1)
-    W = w[:, _OFF[:, 0], 0] * w[:, _OFF[:, 1], 1] * w[:, _OFF[:, 2], 2]
+    off = _OFF.to(x.device)
+    W = w[:, off[:, 0], 0] * w[:, off[:, 1], 1] * w[:, off[:, 2], 2]
     return base, fx, w, W
 
 
 def stencil_nodes(base: torch.Tensor, n_grid: int) -> torch.Tensor:
     """Flat (i*G + j)*G + k index of the 27 nodes of each stencil, shape (N, 27)."""
-    node = base[:, None, :] + _OFF[None]
+    node = base[:, None, :] + _OFF.to(base.device)[None]
     if (node.min() < 0) or (node.max() >= n_grid):
         raise ValueError("particle stencil leaves the grid (reference would index out of bounds)")
     return (node[..., 0] * n_grid + node[..., 1]) * n_grid + node[..., 2]
@@ -336,10 +337,11 @@ class OracleSim:
     # ---------------------------------------------------------------- init
     @staticmethod
     def initialize(const: Constants, vertices, triangles, operator_x=None, cube_x=None,
-                   dtype=torch.float64, svd_grad="exact"):
-        """initialize_ti_field of simulation.py:447-477; returns (sim, state0)."""
-        vx = torch.as_tensor(np.asarray(vertices), dtype=dtype)
-        tris = torch.as_tensor(np.asarray(triangles), dtype=torch.long)
+                   dtype=torch.float64, svd_grad="exact", device=None):
+        """initialize_ti_field of simulation.py:447-477; returns (sim, state0).
+        ``device``: where the state lives (the CPU by default)."""
+        vx = torch.as_tensor(np.asarray(vertices), dtype=dtype, device=device)
+        tris = torch.as_tensor(np.asarray(triangles), dtype=torch.long, device=device)
         a, b, c = vx[tris[:, 0]], vx[tris[:, 1]], vx[tris[:, 2]]
         d1 = b - a
         d2 = c - a
@@ -350,15 +352,16 @@ class OracleSim:
         D0 = torch.stack((d1, d2, d3), dim=-1)
         D0inv = torch.linalg.inv(D0)
         Nv, Nt = vx.shape[0], tris.shape[0]
-        ox = torch.as_tensor(np.zeros((0, 3)) if operator_x is None else np.asarray(operator_x), dtype=dtype)
-        cx = torch.as_tensor(np.zeros((0, 3)) if cube_x is None else np.asarray(cube_x), dtype=dtype)
-        eye = torch.eye(3, dtype=dtype)
+        kw = dict(dtype=dtype, device=device)
+        ox = torch.as_tensor(np.zeros((0, 3)) if operator_x is None else np.asarray(operator_x), **kw)
+        cx = torch.as_tensor(np.zeros((0, 3)) if cube_x is None else np.asarray(cube_x), **kw)
+        eye = torch.eye(3, **kw)
         st = dict(
-            vx=vx, vv=torch.zeros_like(vx), vC=torch.zeros(Nv, 3, 3, dtype=dtype),
-            qx=(a + b + c) / 3, qv=torch.zeros(Nt, 3, dtype=dtype), qC=torch.zeros(Nt, 3, 3, dtype=dtype),
+            vx=vx, vv=torch.zeros_like(vx), vC=torch.zeros(Nv, 3, 3, **kw),
+            qx=(a + b + c) / 3, qv=torch.zeros(Nt, 3, **kw), qC=torch.zeros(Nt, 3, 3, **kw),
             qF=eye.expand(Nt, 3, 3).clone(), qd=D0,
-            ox=ox, ov=torch.zeros_like(ox), oC=torch.zeros(ox.shape[0], 3, 3, dtype=dtype),
-            cx=cx, cv=torch.zeros_like(cx), cC=torch.zeros(cx.shape[0], 3, 3, dtype=dtype),
+            ox=ox, ov=torch.zeros_like(ox), oC=torch.zeros(ox.shape[0], 3, 3, **kw),
+            cx=cx, cv=torch.zeros_like(cx), cC=torch.zeros(cx.shape[0], 3, 3, **kw),
         )
         return OracleSim(const, tris, D0inv, dtype, svd_grad), st
 
@@ -372,7 +375,8 @@ class OracleSim:
         k = self.const
         G, dx, inv_dx, dt = k.n_grid, k.dx, k.inv_dx, k.dt
         dtype = self.dtype
-        off_f = _OFF.to(dtype)
+        dev = st["vx"].device
+        off_f = _OFF.to(dtype=dtype, device=dev)
         E, nu, ks, kc = params["E"], params["nu"], params["ks"], params["kc"]
 
         idx_list, mom_list, mass_list = [], [], []
@@ -396,11 +400,11 @@ class OracleSim:
             affine = k.operator_p_mass * st["oC"]
             frame = keyframe_index(f, dt, k.operator_update_interval, k.frames_per_window, window)
             No = st["ox"].shape[0]
-            gid = torch.arange(No) // k.grasper_group_size
+            gid = torch.arange(No, device=dev) // k.grasper_group_size
             if frame + 1 < k.n_actions:
                 vt = (seq[frame + 1, gid] - seq[frame, gid]) / k.operator_update_interval
             else:
-                vt = torch.zeros(No, 3, dtype=dtype)
+                vt = torch.zeros(No, 3, dtype=dtype, device=dev)
             scatter(stencil_nodes(base, G),
                     W[..., None] * (k.operator_p_mass * vt[:, None, :]
                                     + torch.einsum("nij,nsj->nsi", affine, dpos)),
@@ -409,7 +413,7 @@ class OracleSim:
         vbase, vfx, vw, vW = stencil(st["vx"], inv_dx)
         vnodes = stencil_nodes(vbase, G)
         dpos = (off_f[None] - vfx[:, None, :]) * dx
-        temp_v = st["vv"] + torch.tensor([0.0, k.gravity_dv, 0.0], dtype=dtype)
+        temp_v = st["vv"] + torch.tensor([0.0, k.gravity_dv, 0.0], dtype=dtype, device=dev)
         affine = k.vertex_p_mass * st["vC"]
         scatter(vnodes, vW[..., None] * (k.vertex_p_mass * temp_v[:, None, :]
                                          + torch.einsum("nij,nsj->nsi", affine, dpos)),
@@ -418,7 +422,7 @@ class OracleSim:
         qbase, qfx, qw, qW = stencil(st["qx"], inv_dx)
         qnodes = stencil_nodes(qbase, G)
         xj = torch.stack((qfx - 1.5, 2 * (1.0 - qfx), qfx - 0.5), dim=1) * inv_dx   # (N, 3, 3)
-        o = _OFF
+        o = _OFF.to(dev)
         gw = torch.stack((xj[:, o[:, 0], 0] * qw[:, o[:, 1], 1] * qw[:, o[:, 2], 2],
                           qw[:, o[:, 0], 0] * xj[:, o[:, 1], 1] * qw[:, o[:, 2], 2],
                           qw[:, o[:, 0], 0] * qw[:, o[:, 1], 1] * xj[:, o[:, 2], 2]), dim=-1)  # (N,27,3)
@@ -445,8 +449,8 @@ class OracleSim:
         # --- grid (only touched nodes are materialised)
         flat = torch.cat(idx_list)
         uniq, inv = torch.unique(flat, return_inverse=True)
-        gp = torch.zeros(uniq.shape[0], 3, dtype=dtype).index_add(0, inv, torch.cat(mom_list))
-        gm = torch.zeros(uniq.shape[0], dtype=dtype).index_add(0, inv, torch.cat(mass_list))
+        gp = torch.zeros(uniq.shape[0], 3, dtype=dtype, device=dev).index_add(0, inv, torch.cat(mom_list))
+        gm = torch.zeros(uniq.shape[0], dtype=dtype, device=dev).index_add(0, inv, torch.cat(mass_list))
         node_xyz = torch.stack((uniq // (G * G), (uniq // G) % G, uniq % G), -1)
         gv = grid_op(gp, gm, node_xyz, G, k.bound, friction=friction, grip=grip, f=f, dx=dx)
         lookup = {}

@@ -29,7 +29,7 @@ def reference_small_scene():
     return sc
 
 
-def oracle_for(sc: dscene.ClothScene, dtype=torch.float64, svd_grad="exact"):
+def oracle_for(sc: dscene.ClothScene, dtype=torch.float64, svd_grad="exact", device=None):
     """Oracle simulator + state 0 for a product scene."""
     const = Constants(
         n_grid=sc.n_grid, dt=float(sc.meta["dt"]), vertex_p_mass=sc.vertex_p_mass,
@@ -38,7 +38,7 @@ def oracle_for(sc: dscene.ClothScene, dtype=torch.float64, svd_grad="exact"):
         operator_update_interval=sc.keyframe_interval, frames_per_window=sc.frames_per_window,
         grasper_group_size=max(sc.group_size, 1), n_actions=0 if sc.keyframes is None else sc.keyframes.shape[0])
     return OracleSim.initialize(const, sc.vertices, sc.triangles, sc.operator_x, sc.cube_x, dtype=dtype,
-                                svd_grad=svd_grad)
+                                svd_grad=svd_grad, device=device)
 
 
 def oracle_params(sc, dtype=torch.float64, requires_grad=False):
