@@ -145,8 +145,8 @@ void make_layout(const DcpInstance* in, int n, const DcpOptions* opt, Layout& L)
   L.off_lblk = o; o = align256(o + 4 * blocks);
   L.off_linst = o; o = align256(o + 4 * blocks);
   L.off_cnt = o; o = align256(o + 64);
-  L.off_force = o; o = align256(o + 4 * 9 * L.nt);
-  L.off_contrib = o; o = align256(o + 4 * 18 * L.nt);
+  L.off_force = o; o = align256(o + 16 * L.nv);
+  L.off_contrib = o; o = align256(o + 32 * L.nv);
   L.off_barf = o; o = align256(o + 4 * 3 * L.nv);
   L.off_tmp = o; o = align256(o + 4 * 3 * L.nt);
   L.off_status = o; o = align256(o + 4 * n);
@@ -282,8 +282,8 @@ int dcp_create(const DcpInstance* inst, int32_t n_inst, const DcpOptions* opt, c
   B.list_blk = (int*)(wd + L.off_lblk);
   B.list_inst = (int*)(wd + L.off_linst);
   B.counters = (int*)(wd + L.off_cnt);
-  B.force = (float*)(wd + L.off_force);
-  B.contrib = (float*)(wd + L.off_contrib);
+  B.fvert = (float4*)(wd + L.off_force);
+  B.vadj = (float4*)(wd + L.off_contrib);
   B.barf = (float*)(wd + L.off_barf);
   B.tri_tmp = (float*)(wd + L.off_tmp);
   B.status = (int*)(wd + L.off_status);
@@ -569,8 +569,11 @@ int dcp_rollout_backward(DcpBatch* b, const float* params, const float* traj, co
       }
       for (int f = last; f >= f0; --f) {
         const int so = (Lstep - 1 - f) % 2;
+        // state f + 1: inside the segment, or the next checkpoint / final state
+        const long long nslot = f < last ? -2 : ckpt_slot(f + 1, n, K);
+        const float* snext = f < last ? state_at(f + 1) : (nslot >= 0 ? buf + nslot * S : nullptr);
         cudaError_t e = launch_backward(b->B, b->L, params, traj, rest, f, window, state_at(f), adj + so * S,
-                                        adj + (1 - so) * S, gparams, gtraj, s, tp);
+                                        adj + (1 - so) * S, gparams, gtraj, s, tp, snext);
         if (e != cudaSuccess) return e;
       }
     }

@@ -69,8 +69,8 @@ struct BatchDev {
   int* list_blk;
   int* list_inst;
   int* counters;  // [0] active blocks
-  float* force;   // [3][3 nt]
-  float* contrib; // [6][3 nt]
+  float4* fvert;  // [nv] summed in-plane corner forces of each vertex (xyz, w unused)
+  float4* vadj;   // [2][nv] per-vertex sums of the triangles' position / velocity adjoints
   float* barf;    // [3][nv]
   float* tri_tmp; // [3][nt]
   int* status;    // [n_inst]

@@ -79,9 +79,12 @@ cudaError_t launch_forward(const BatchDev& B, const LaunchCfg& L, const float* p
                            const TapeP* T = nullptr, const float* fdev = nullptr);
 cudaError_t launch_reset(const BatchDev& B, const LaunchCfg& L, float* rest, float* state, float* fdev,
                          cudaStream_t s);
+// snext (optional): the state after this substep, as the forward produced it;
+// the triangles' damped C is read from it instead of being gathered again.
 cudaError_t launch_backward(const BatchDev& B, const LaunchCfg& L, const float* params, const float* traj,
                             const float* rest, int step, int window, const float* sin, const float* aout, float* ain,
-                            double* gparams, double* gtraj, cudaStream_t s, const TapeP* T = nullptr);
+                            double* gparams, double* gtraj, cudaStream_t s, const TapeP* T = nullptr,
+                            const float* snext = nullptr);
 cudaError_t launch_chamfer_forward(const BatchDev& B, const LaunchCfg& L, int max_nq, const float* rest,
                                    const float* state, const float* targets, int* qarg, float* loss, cudaStream_t s);
 cudaError_t launch_chamfer_backward(const BatchDev& B, const LaunchCfg& L, int max_nq, const float* rest,

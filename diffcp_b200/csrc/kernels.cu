@@ -6,8 +6,8 @@
 //   k_tri_forward    in-plane QR + rotation factor + stress of every triangle
 //                    (simulation.py:24-28, 39-42, 214-240), its own-node APIC
 //                    scatter and normal force (simulation.py:193-265), and the
-//                    per-corner in-plane forces (simulation.py:266-271) written
-//                    to a buffer instead of being scattered at the vertices'
+//                    per-corner in-plane forces (simulation.py:266-271) summed
+//                    per vertex instead of being scattered at the vertices'
 //                    stencils (see k_point_p2g)
 //   k_point_p2g      vertex / operator / cube APIC scatter (simulation.py:139-191);
 //                    a vertex adds the sum of its triangles' corner forces, which
@@ -223,10 +223,11 @@ __global__ void __launch_bounds__(256, MINB) k_tri_forward(BatchDev B, const flo
     const V3<float> f1 = k * matvec(P, r1 + r2);
     const V3<float> f2 = (-k) * matvec(P, r1);
     const V3<float> f3 = (-k) * matvec(P, r2);
-    const long long e3 = 3 * nt;
-    B.force[0 * e3 + 0 * nt + t] = f1.x; B.force[1 * e3 + 0 * nt + t] = f1.y; B.force[2 * e3 + 0 * nt + t] = f1.z;
-    B.force[0 * e3 + 1 * nt + t] = f2.x; B.force[1 * e3 + 1 * nt + t] = f2.y; B.force[2 * e3 + 1 * nt + t] = f2.z;
-    B.force[0 * e3 + 2 * nt + t] = f3.x; B.force[1 * e3 + 2 * nt + t] = f3.y; B.force[2 * e3 + 2 * nt + t] = f3.z;
+    // summed per vertex (one vector reduction per corner); the vertex scatter
+    // of k_point_p2g reads the sums
+    atomicAdd(B.fvert + g.vid[0], make_float4(f1.x, f1.y, f1.z, 0.f));
+    atomicAdd(B.fvert + g.vid[1], make_float4(f2.x, f2.y, f2.z, 0.f));
+    atomicAdd(B.fvert + g.vid[2], make_float4(f3.x, f3.y, f3.z, 0.f));
     const float cn = -vol * dt;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -282,7 +283,8 @@ __device__ __forceinline__ bool operator_velocity(const BatchDev& B, const InstD
 
 __global__ void __launch_bounds__(256) k_point_p2g(BatchDev B, const float* __restrict__ traj, int step, int window,
                                                    const float* __restrict__ rest, const float* __restrict__ sin,
-                                                   const int2* __restrict__ skip, float* __restrict__ fv_out) {
+                                                   const int2* __restrict__ skip, float* __restrict__ fv_out,
+                                                   int clear_forces) {
   if (skip && skip->x >= 0) return;  // the grid of this substep is restored from the tape
   const Chunk ch = B.chunks[B.n_tri_chunks + blockIdx.x];
   const InstDev& I = B.inst[ch.inst];
@@ -303,14 +305,8 @@ __global__ void __launch_bounds__(256) k_point_p2g(BatchDev B, const float* __re
     for (int a = 0; a < 3; ++a) X[a] = __ldg(x0 + a * n + p) + __ldg(arr + a * n + p);
     make_stencil(X, I, st, B.status, ch.inst);
     if (ch.kind == CHUNK_VERTEX) {
-      float f[3] = {0.f, 0.f, 0.f};
-      const long long e3 = 3LL * B.nt;
-      const int e0 = __ldg(B.inc_ptr + p), e1 = __ldg(B.inc_ptr + p + 1);
-      for (int e = e0; e < e1; ++e) {
-        const int id = __ldg(B.inc_e + e);
-#pragma unroll
-        for (int a = 0; a < 3; ++a) f[a] += B.force[a * e3 + id];
-      }
+      const float4 fs = B.fvert[p];
+      const float f[3] = {fs.x, fs.y, fs.z};
       if (fv_out) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) fv_out[a * (long long)B.nv + p] = f[a];
@@ -339,6 +335,8 @@ __global__ void __launch_bounds__(256) k_point_p2g(BatchDev B, const float* __re
     val.w = W * m;
     return val;
   });
+  // cleared after all loads of the kernel, ready for the next substep's sums
+  if (clear_forces && valid && ch.kind == CHUNK_VERTEX) B.fvert[p] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
 // Node coordinates of lane l (0..63) of an active block.
@@ -541,7 +539,7 @@ template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* __restrict__ params,
                                                  const float* __restrict__ rest, const float* __restrict__ sin,
                                                  const float* __restrict__ aout, float* __restrict__ ain,
-                                                 double* __restrict__ gparams) {
+                                                 double* __restrict__ gparams, const float* __restrict__ snext) {
   const Chunk ch = B.chunks[blockIdx.x];
   const InstDev& I = B.inst[ch.inst];
   const int tid = threadIdx.x;
@@ -577,32 +575,45 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
     float bx[3] = {0.f, 0.f, 0.f};
     if (tri) {
       const long long nt = B.nt;
-      float Ct[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      const float4* gnb = B.grid_v + I.node_off;
-      const NodeOffsets nofs = node_offsets(I, st.base);
-#pragma unroll
-      for (int q = 0; q < 27; ++q) {
-        const int oi = q / 9, oj = (q / 3) % 3, ok = q % 3;
-        const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
-        const float dp[3] = {(float)oi - st.fx[0], (float)oj - st.fx[1], (float)ok - st.fx[2]};
-        const float3 gn = gv_at(gnb, nofs, oi, oj, ok);
-        const float ga[3] = {gn.x, gn.y, gn.z};
-        const float s = 4.f * W * inv_dx;
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-          for (int b = 0; b < 3; ++b) Ct[3 * a + b] += s * ga[a] * dp[b];
-      }
       const float damping = __ldg(params + ch.inst * PRM_STRIDE + PRM_DAMPING);
       const float keep = 1.f - damping;
       float Cn[9], sym[9];
+      if (snext && keep > 0.f) {
+        // the damped C of the forward is the next state's C; its symmetric
+        // part is keep times that of the gathered C (uniform per chunk)
+        const float* cn = snext + 15LL * B.nv;
 #pragma unroll
-      for (int a = 0; a < 3; ++a)
+        for (int q = 0; q < 9; ++q) Cn[q] = __ldg(cn + q * nt + idx);
+        const float ik = 1.f / keep;
 #pragma unroll
-        for (int b = 0; b < 3; ++b) {
-          sym[3 * a + b] = 0.5f * (Ct[3 * a + b] + Ct[3 * b + a]);
-          Cn[3 * a + b] = 0.5f * (Ct[3 * a + b] - Ct[3 * b + a]) + keep * sym[3 * a + b];
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int b = 0; b < 3; ++b) sym[3 * a + b] = 0.5f * (Cn[3 * a + b] + Cn[3 * b + a]) * ik;
+      } else {
+        float Ct[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        const float4* gnb = B.grid_v + I.node_off;
+        const NodeOffsets nofs = node_offsets(I, st.base);
+#pragma unroll
+        for (int q = 0; q < 27; ++q) {
+          const int oi = q / 9, oj = (q / 3) % 3, ok = q % 3;
+          const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
+          const float dp[3] = {(float)oi - st.fx[0], (float)oj - st.fx[1], (float)ok - st.fx[2]};
+          const float3 gn = gv_at(gnb, nofs, oi, oj, ok);
+          const float ga[3] = {gn.x, gn.y, gn.z};
+          const float s = 4.f * W * inv_dx;
+#pragma unroll
+          for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) Ct[3 * a + b] += s * ga[a] * dp[b];
         }
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int b = 0; b < 3; ++b) {
+            sym[3 * a + b] = 0.5f * (Ct[3 * a + b] + Ct[3 * b + a]);
+            Cn[3 * a + b] = 0.5f * (Ct[3 * a + b] - Ct[3 * b + a]) + keep * sym[3 * a + b];
+          }
+      }
       float d3[3], bd3o[3], bCo[9];
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
@@ -786,14 +797,9 @@ __global__ void __launch_bounds__(256) k_point_adj(BatchDev B, const float* __re
     if (fv_in && tmeta->x >= 0) {  // summed corner forces kept by the forward substep
 #pragma unroll
       for (int a = 0; a < 3; ++a) f[a] = __ldg(fv_in + a * (long long)B.nv + p);
-    } else {
-      const long long e3 = 3LL * B.nt;
-      const int e0 = __ldg(B.inc_ptr + p), e1 = __ldg(B.inc_ptr + p + 1);
-      for (int e = e0; e < e1; ++e) {
-        const int id = __ldg(B.inc_e + e);
-#pragma unroll
-        for (int a = 0; a < 3; ++a) f[a] += B.force[a * e3 + id];
-      }
+    } else {  // recomputed by this substep's k_tri_forward; cleared at the end of this kernel
+      const float4 fs = B.fvert[p];
+      f[0] = fs.x; f[1] = fs.y; f[2] = fs.z;
     }
     base_v[0] = m * __ldg(ai + 3 * n + p) + f[0];
     base_v[1] = m * (__ldg(ai + 4 * n + p) + I.gravity_dv) + f[1];
@@ -850,6 +856,7 @@ __global__ void __launch_bounds__(256) k_point_adj(BatchDev B, const float* __re
       aa[(3 + a) * n + p] = m * sp[a];
       B.barf[a * (long long)B.nv + p] = sp[a];
     }
+    if (!(fv_in && tmeta->x >= 0)) B.fvert[p] = make_float4(0.f, 0.f, 0.f, 0.f);  // for the next sums
   } else {
 #pragma unroll
     for (int a = 0; a < 3; ++a) aa[(3 + a) * n + p] = 0.f;
@@ -868,8 +875,8 @@ __global__ void __launch_bounds__(256) k_point_adj(BatchDev B, const float* __re
 
 // Reverse of k_tri_forward for one triangle: own-stencil gather, per-corner
 // force adjoints from dL/df of the three vertices, stress adjoint, and the
-// contributions to the three vertices (written per corner, summed by
-// k_vertex_collect).
+// contributions to the three vertices (summed per vertex, added to the vertex
+// adjoint by k_vertex_collect).
 template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* __restrict__ params,
                                                  const float* __restrict__ rest, const float* __restrict__ sin,
@@ -993,17 +1000,15 @@ __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* 
     float bxt[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) bxt[a] = third * (bx[a] + B.tri_tmp[a * nt + t]);
-    const long long e3 = 3 * nt;
+    // per-vertex sums of the corners' position and velocity adjoints
+    const float4 bvc = make_float4(third * m * sp[0], third * m * sp[1], third * m * sp[2], 0.f);
+    const long long nv = B.nv;
+    atomicAdd(B.vadj + g.vid[0], make_float4(bxt[0] - be1[0] - be2[0], bxt[1] - be1[1] - be2[1],
+                                             bxt[2] - be1[2] - be2[2], 0.f));
+    atomicAdd(B.vadj + g.vid[1], make_float4(bxt[0] + be1[0], bxt[1] + be1[1], bxt[2] + be1[2], 0.f));
+    atomicAdd(B.vadj + g.vid[2], make_float4(bxt[0] + be2[0], bxt[1] + be2[1], bxt[2] + be2[2], 0.f));
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      B.contrib[a * e3 + 0 * nt + t] = bxt[a] - be1[a] - be2[a];
-      B.contrib[a * e3 + 1 * nt + t] = bxt[a] + be1[a];
-      B.contrib[a * e3 + 2 * nt + t] = bxt[a] + be2[a];
-      const float bvc = third * m * sp[a];
-      B.contrib[(3 + a) * e3 + 0 * nt + t] = bvc;
-      B.contrib[(3 + a) * e3 + 1 * nt + t] = bvc;
-      B.contrib[(3 + a) * e3 + 2 * nt + t] = bvc;
-    }
+    for (int c = 0; c < 3; ++c) atomicAdd(B.vadj + nv + g.vid[c], bvc);
 #pragma unroll
     for (int q = 0; q < 9; ++q) Ai.t[q * nt + t] = m * spd[q];
 #pragma unroll
@@ -1022,20 +1027,17 @@ __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* 
 
 __global__ void k_vertex_collect(BatchDev B, float* __restrict__ ain) {
   StateP Ai = state_ptrs(ain, B.nv, B.nt, B.no);
-  const long long e3 = 3LL * B.nt, nv = B.nv;
+  const long long nv = B.nv;
   for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nv; v += (long long)gridDim.x * blockDim.x) {
-    float s[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    const int e0 = __ldg(B.inc_ptr + v), e1 = __ldg(B.inc_ptr + v + 1);
-    for (int e = e0; e < e1; ++e) {
-      const int id = __ldg(B.inc_e + e);
-#pragma unroll
-      for (int q = 0; q < 6; ++q) s[q] += B.contrib[q * e3 + id];
-    }
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      Ai.v[a * nv + v] += s[a];
-      Ai.v[(3 + a) * nv + v] += s[3 + a];
-    }
+    const float4 bx = B.vadj[v], bv = B.vadj[nv + v];
+    Ai.v[v] += bx.x;
+    Ai.v[nv + v] += bx.y;
+    Ai.v[2 * nv + v] += bx.z;
+    Ai.v[3 * nv + v] += bv.x;
+    Ai.v[4 * nv + v] += bv.y;
+    Ai.v[5 * nv + v] += bv.z;
+    B.vadj[v] = make_float4(0.f, 0.f, 0.f, 0.f);       // ready for the next substep's sums
+    B.vadj[nv + v] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
 }
 
@@ -1276,7 +1278,7 @@ cudaError_t launch_forward(const BatchDev& B, const LaunchCfg& L, const float* p
   if (B.n_point_chunks)
     DCP_LAUNCH(KID_POINT_P2G, (k_point_p2g<<<B.n_point_chunks, L.block, 0, s>>>(
                                   B, traj, step, window, rest, sin, nullptr,
-                                  T ? tp.fv + (long long)step * 3 * B.nv : nullptr)));
+                                  T ? tp.fv + (long long)step * 3 * B.nv : nullptr, 1)));
   if (T) DCP_LAUNCH(KID_TAPE, (k_tape_reserve<<<1, 32, 0, s>>>(B, tp, step)));
   DCP_LAUNCH(KID_GRID, (k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_FORWARD, tp)));
   if (B.n_tri_chunks)
@@ -1288,7 +1290,7 @@ cudaError_t launch_forward(const BatchDev& B, const LaunchCfg& L, const float* p
 
 cudaError_t launch_backward(const BatchDev& B, const LaunchCfg& L, const float* params, const float* traj,
                             const float* rest, int step, int window, const float* sin, const float* aout, float* ain,
-                            double* gparams, double* gtraj, cudaStream_t s, const TapeP* T) {
+                            double* gparams, double* gtraj, cudaStream_t s, const TapeP* T, const float* snext) {
   const TapeP none = no_tape();
   const int2* meta = T ? T->meta + step : nullptr;
   cudaMemsetAsync(B.counters, 0, sizeof(int), s);
@@ -1298,10 +1300,10 @@ cudaError_t launch_backward(const BatchDev& B, const LaunchCfg& L, const float* 
                                     B, params, rest, sin, meta, nullptr)));
   if (B.n_point_chunks)
     DCP_LAUNCH(KID_POINT_P2G, (k_point_p2g<<<B.n_point_chunks, L.block, 0, s>>>(B, traj, step, window, rest, sin,
-                                                                               meta, nullptr)));
+                                                                               meta, nullptr, 0)));
   DCP_LAUNCH(KID_GRID, (k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_RECOMPUTE, none)));
   DCP_LAUNCH(KID_G2P_ADJ, (DCP_MINB(k_g2p_adj, L, 1)<<<B.n_tri_chunks + B.n_point_chunks, L.block, 0, s>>>(
-                              B, params, rest, sin, aout, ain, gparams)));
+                              B, params, rest, sin, aout, ain, gparams, snext)));
   DCP_LAUNCH(KID_GRID_ADJ, (k_grid_adj<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, gparams, gtraj)));
   if (B.n_point_chunks)
     DCP_LAUNCH(KID_POINT_ADJ, (k_point_adj<<<B.n_point_chunks, L.block, 0, s>>>(
