@@ -151,10 +151,11 @@ def counts(scenes):
 
 
 # ------------------------------------------------------------------ CPU
-def cpu_rate(scenes, info, seconds=15.0):
+def cpu_rate(scenes, info, seconds=15.0, steps=1, warmup=0):
     """Oracle (torch, float32, all host threads) fwd+bwd rate on a bounded
-    sample of the workload: the instance nearest the median size, as many
-    substeps as fit in about ``seconds``."""
+    sample of the workload: the instance nearest the median size; each of
+    ``steps`` timed steps runs as many substeps as fit in about
+    ``seconds / steps`` (after ``warmup`` short untimed steps)."""
     import torch
     from oracle import sim64
     from oracle.sim64 import Constants, KinematicGripper, OracleSim
@@ -179,40 +180,48 @@ def cpu_rate(scenes, info, seconds=15.0):
     t0 = time.perf_counter()
     run(2)
     per = (time.perf_counter() - t0) / 2
-    n = int(max(2, min(info["n_steps"], seconds / max(per, 1e-3))))
+    # one step = fwd+bwd of n substeps, n sized so that the timed steps take about `seconds`
+    n = int(max(2, min(info["n_steps"], seconds / max(steps, 1) / max(per, 1e-3))))
+    for _ in range(warmup):
+        run(2)
     t0 = time.perf_counter()
-    run(n)
+    for _ in range(max(steps, 1)):
+        run(n)
     el = time.perf_counter() - t0
-    rate = (sc.n_vertex + sc.n_tri) * n / el
+    k = max(steps, 1)
+    rate = (sc.n_vertex + sc.n_tri) * n * k / el
     return {"value": rate, "unit": UNIT, "cores": torch.get_num_threads(), "kind": "port",
+            "ms_per_step": 1e3 * el / k,
             "sample": "CPU oracle (torch float32) fwd+bwd of %d substeps of one %d-vertex/%d-triangle cloth of the "
-                      "workload, %.1f s" % (n, sc.n_vertex, sc.n_tri, el)}
+                      "workload per step, %d step(s) in %.1f s" % (n, sc.n_vertex, sc.n_tri, k, el)}
 
 
 def profile_substeps(args):
-    """A few eager substeps and adjoint substeps of the workload on a handful
-    of state buffers (a few GB on the device), for kernel profilers."""
+    """Two eager rollouts of ``args.profile_substeps`` substeps of the workload
+    (forward, Chamfer, adjoint) through the same path as the bench: the first
+    sizes the grid tape, the second restores from it and reads the next
+    state's C in the adjoint.  A few GB on the device; for kernel profilers.
+    Launch order of the second rollout, per substep: forward k_tri_forward,
+    k_point_p2g, k_tape_reserve, k_grid, k_g2p x2; adjoint k_tape_restore,
+    k_tri_forward and k_point_p2g (both return at once), k_grid, k_g2p_adj,
+    k_grid_adj, k_point_adj, k_tri_adj, k_vertex_collect."""
     import torch
     from diffcp_b200 import autotune
-    from diffcp_b200.batch import ClothBatch
+    from diffcp_b200.batch import BatchSim, ClothBatch
     scenes, info = workload(args.workload, 0)
     cache = args.tune_cache or autotune.CACHE
     launch = (autotune.cached(scenes, info["dt"], cache=cache) if os.path.exists(cache) else None) or autotune.DEFAULT
     b = ClothBatch(scenes, dt=info["dt"], chunk=launch["chunk"], scatter_mode=launch["scatter_mode"],
                    min_blocks=launch["min_blocks"])
     n = args.profile_substeps
-    states = [b.init_state()]
-    for f in range(n):
-        states.append(b.forward_step(states[-1], f))
-    gp, gt = b.new_grads()
-    adj = torch.zeros(b.S, device=b.device)
-    loss, arg = b.chamfer(states[-1])
-    b.chamfer_backward(states[-1], arg, torch.ones_like(loss), adj)
-    for f in range(n - 1, -1, -1):
-        adj = b.backward_step(states[f], adj, f, gp, gt)
+    sim = BatchSim(b, n_steps=n, ckpt_every=1, use_graph=False, tape="auto")
+    for _ in range(2):
+        params = b.params.clone().requires_grad_(True)
+        traj = b.traj.clone().requires_grad_(True)
+        sim.loss(params, traj).sum().backward()
     torch.cuda.synchronize()
     st = b.status()
-    print(json.dumps({"profile_substeps": n, "instances": len(scenes), "finite": bool(torch.isfinite(adj).all()),
+    print(json.dumps({"profile_substeps": n, "instances": len(scenes), "finite": bool(torch.isfinite(params.grad).all()),
                       "status_nonzero": int((st != 0).sum())}))
 
 
@@ -241,9 +250,9 @@ def main():
         if rank != 0:
             return
         scenes, info = workload(args.workload, 0)
-        cb = cpu_rate(scenes, info, seconds=max(args.cpu_seconds, 5.0))
+        cb = cpu_rate(scenes, info, seconds=max(args.cpu_seconds, 5.0), steps=args.steps, warmup=args.warmup)
         line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                "warmup": args.warmup, "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
                 "config": {"workload": info["desc"]}, "cpu_baseline": cb,
                 "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -306,12 +315,15 @@ def main():
     barrier()
     ms = e0.elapsed_time(e1) / args.steps
     launches = (batch.launch_count() - launches0) // max(args.steps, 1)
-    t = torch.tensor([ms], device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(t.item())
+    from diffcp_b200 import sharding
+    ms_max = sharding.max_over_ranks(ms, device=dev)
     psteps = (nv + nt) * info["n_steps"]
-    value = psteps * world / (ms_max / 1e3)
+    # every rank simulates its own workload copy: the job's units are the sum over ranks
+    units = torch.tensor([float(psteps)], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(units)
+    job_psteps = float(units.item())
+    value = job_psteps / (ms_max / 1e3)
 
     # ---- e2e: public API with host buffers (pinned H2D of the inputs, D2H of loss and gradients)
     h_params = params.detach().cpu().pin_memory()
@@ -345,10 +357,8 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     ms_e2e = e0.elapsed_time(e1) / args.steps
-    t = torch.tensor([ms_e2e], device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    e2e_val = psteps * world / (float(t.item()) / 1e3)
+    ms_e2e_max = sharding.max_over_ranks(ms_e2e, device=dev)
+    e2e_val = job_psteps / (ms_e2e_max / 1e3)
     h2d = (h_params.numel() + h_traj.numel() + h_targets.numel()) * 4
     d2h = (h_loss.numel() + h_gp.numel() + h_gt.numel()) * 4
 
@@ -430,7 +440,7 @@ def main():
         "cpu_baseline": cpu,
         "single_instance": single,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "ms_per_step": float(t.item())},
+                "ms_per_step": ms_e2e_max},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "status_nonzero_instances": int((status != 0).sum()),

@@ -44,7 +44,7 @@ struct Layout {
   long long nv = 0, nt = 0, no = 0, nc = 0, nq = 0, total_nodes = 0, traj = 0;
   int max_nq = 0;
   // static buffer offsets
-  size_t off_inst, off_triv, off_incptr, off_ince, off_chunks, off_rank, static_bytes;
+  size_t off_inst, off_triv, off_chunks, off_rank, static_bytes;
   // workspace offsets
   size_t off_pm, off_v, off_adj, off_flags, off_lblk, off_linst, off_cnt, off_force, off_contrib, off_barf, off_tmp,
       off_status, off_qmin, ws_bytes;
@@ -131,8 +131,6 @@ void make_layout(const DcpInstance* in, int n, const DcpOptions* opt, Layout& L)
   size_t o = 0;
   L.off_inst = o; o = align256(o + sizeof(InstDev) * n);
   L.off_triv = o; o = align256(o + sizeof(int) * 3 * L.nt);
-  L.off_incptr = o; o = align256(o + sizeof(int) * (L.nv + 1));
-  L.off_ince = o; o = align256(o + sizeof(int) * 3 * L.nt);
   L.off_chunks = o; o = align256(o + sizeof(Chunk) * L.chunks.size());
   L.off_rank = o; o = align256(o + sizeof(int) * L.nv);
   L.static_bytes = o;
@@ -220,7 +218,7 @@ int dcp_create(const DcpInstance* inst, int32_t n_inst, const DcpOptions* opt, c
   make_layout(inst, n_inst, opt, L);
   fill_sizes(L, n_inst, &b->sizes);
   // host tables
-  std::vector<int> triv(3 * L.nt), incptr(L.nv + 1, 0), ince(3 * L.nt), rank(L.nv);
+  std::vector<int> triv(3 * L.nt), rank(L.nv);
   for (int i = 0; i < n_inst; ++i) {
     const InstDev& I = L.inst[i];
     for (int t = 0; t < I.nt; ++t)
@@ -233,22 +231,12 @@ int dcp_create(const DcpInstance* inst, int32_t n_inst, const DcpOptions* opt, c
         triv[(long long)c * L.nt + I.t_off + t] = I.v_off + v;
       }
   }
-  for (long long t = 0; t < L.nt; ++t)
-    for (int c = 0; c < 3; ++c) incptr[triv[c * L.nt + t] + 1]++;
-  for (long long v = 0; v < L.nv; ++v) incptr[v + 1] += incptr[v];
-  {
-    std::vector<int> fill(incptr.begin(), incptr.end() - 1);
-    for (int c = 0; c < 3; ++c)
-      for (long long t = 0; t < L.nt; ++t) ince[fill[triv[c * L.nt + t]]++] = (int)(c * L.nt + t);
-  }
   for (int i = 0; i < n_inst; ++i)
     for (int v = 0; v < L.inst[i].nv; ++v)
       rank[L.inst[i].v_off + v] = vertex_rank ? vertex_rank[L.inst[i].v_off + v] : v;
   std::vector<unsigned char> host(L.static_bytes, 0);
   memcpy(host.data() + L.off_inst, L.inst.data(), sizeof(InstDev) * n_inst);
   memcpy(host.data() + L.off_triv, triv.data(), sizeof(int) * triv.size());
-  memcpy(host.data() + L.off_incptr, incptr.data(), sizeof(int) * incptr.size());
-  memcpy(host.data() + L.off_ince, ince.data(), sizeof(int) * ince.size());
   memcpy(host.data() + L.off_chunks, L.chunks.data(), sizeof(Chunk) * L.chunks.size());
   memcpy(host.data() + L.off_rank, rank.data(), sizeof(int) * rank.size());
   cudaStream_t s = (cudaStream_t)stream;
@@ -266,8 +254,6 @@ int dcp_create(const DcpInstance* inst, int32_t n_inst, const DcpOptions* opt, c
   B.n_inst = n_inst;
   B.nv = (int)L.nv; B.nt = (int)L.nt; B.no = (int)L.no; B.nc = (int)L.nc; B.nq = (int)L.nq;
   B.tri_v = (const int*)(sd + L.off_triv);
-  B.inc_ptr = (const int*)(sd + L.off_incptr);
-  B.inc_e = (const int*)(sd + L.off_ince);
   B.chunks = (const Chunk*)(sd + L.off_chunks);
   B.n_tri_chunks = L.n_tri_chunks;
   B.n_point_chunks = L.n_point_chunks;

@@ -13,7 +13,7 @@
 // (absolute positions near 0.5 would leave ~1e-5 strain resolution).
 //   grid             block-major per instance: 4x4x4-node blocks of 64 nodes,
 //                    float4 (p.xyz, m) / (v_out.xyz, 0) / adjoint per node
-//   topology         [3][Nt] global vertex ids, vertex->(corner, triangle) CSR
+//   topology         [3][Nt] global vertex ids
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -53,8 +53,6 @@ struct BatchDev {
   int n_inst;
   int nv, nt, no, nc, nq;
   const int* tri_v;     // [3][nt]
-  const int* inc_ptr;   // [nv + 1]
-  const int* inc_e;     // [3 nt], e = corner * nt + t
   const Chunk* chunks;  // tri chunks then point chunks
   int n_tri_chunks, n_point_chunks;
   const int* vertex_rank;  // [nv] tie-break rank for the Chamfer argmin

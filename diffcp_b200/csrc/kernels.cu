@@ -678,7 +678,7 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
       for (int q = 0; q < 9; ++q) bC[q] = __ldg(ao + (6 + q) * n + idx);
     }
     // position adjoint of the gather (second pass over the stencil)
-    float px[3] = {0.f, 0.f, 0.f};
+    float px[3] = {0.f, 0.f, 0.f}, vs[3] = {0.f, 0.f, 0.f};
     const float c4 = 4.f * inv_dx;
     const float4* gnb = B.grid_v + I.node_off;
     const NodeOffsets nofs = node_offsets(I, st.base);
@@ -696,10 +696,13 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
       for (int a = 0; a < 3; ++a) s1 += c4 * ga[a] * (bC[3 * a] * dp[0] + bC[3 * a + 1] * dp[1] + bC[3 * a + 2] * dp[2]);
 #pragma unroll
       for (int b = 0; b < 3; ++b) {
-        const float cg = bC[b] * ga[0] + bC[3 + b] * ga[1] + bC[6 + b] * ga[2];
-        px[b] += s1 * gW[b] - c4 * inv_dx * W * cg;
+        px[b] += s1 * gW[b];
+        vs[b] += W * ga[b];
       }
     }
+    // - c4 inv_dx sum_nodes W bC^T g = - c4 inv_dx bC^T (sum_nodes W g)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) px[b] -= c4 * inv_dx * (bC[b] * vs[0] + bC[3 + b] * vs[1] + bC[6 + b] * vs[2]);
     if (tri) {
       const long long nt = B.nt;
 #pragma unroll
@@ -768,7 +771,7 @@ __global__ void __launch_bounds__(256) k_grid_adj(BatchDev B, const float* __res
 }
 
 // Reverse of k_point_p2g: gather dL/dp, dL/dm over the stencil.
-__global__ void __launch_bounds__(256) k_point_adj(BatchDev B, const float* __restrict__ traj, int step, int window,
+__global__ void __launch_bounds__(256, 3) k_point_adj(BatchDev B, const float* __restrict__ traj, int step, int window,
                                                    const float* __restrict__ rest, const float* __restrict__ sin,
                                                    float* __restrict__ ain, double* __restrict__ gtraj,
                                                    const int2* __restrict__ tmeta, const float* __restrict__ fv_in) {
@@ -831,21 +834,20 @@ __global__ void __launch_bounds__(256) k_point_adj(BatchDev B, const float* __re
     const float4 g = __ldg(gnb + (nofs.ax[oi] + nofs.ay[oj] + nofs.az[ok]));
     const float bp[3] = {g.x, g.y, g.z};
     float s = g.w * m;
-    float ctb[3] = {0.f, 0.f, 0.f};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const float pay = base_v[a] + m * (Cm[3 * a] * dp[0] + Cm[3 * a + 1] * dp[1] + Cm[3 * a + 2] * dp[2]);
       s += bp[a] * pay;
       sp[a] += W * bp[a];
 #pragma unroll
-      for (int b = 0; b < 3; ++b) {
-        spd[3 * a + b] += W * bp[a] * dp[b];
-        ctb[b] += Cm[3 * a + b] * bp[a];
-      }
+      for (int b = 0; b < 3; ++b) spd[3 * a + b] += W * bp[a] * dp[b];
     }
 #pragma unroll
-    for (int b = 0; b < 3; ++b) px[b] += s * gW[b] - W * m * ctb[b];
+    for (int b = 0; b < 3; ++b) px[b] += s * gW[b];
   }
+  // - sum_nodes W m C^T bp = - m C^T sp
+#pragma unroll
+  for (int b = 0; b < 3; ++b) px[b] -= m * (Cm[b] * sp[0] + Cm[3 + b] * sp[1] + Cm[6 + b] * sp[2]);
 #pragma unroll
   for (int a = 0; a < 3; ++a) aa[a * n + p] += px[a];
 #pragma unroll
@@ -934,7 +936,6 @@ __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* 
       const float gdot = gW[0] * d3[0] + gW[1] * d3[1] + gW[2] * d3[2];
       const float sP = bp[0] * P3[0] + bp[1] * P3[1] + bp[2] * P3[2];
       float s = ga.w * m;
-      float ctb[3] = {0.f, 0.f, 0.f};
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         const float pay = mv[a] + m * (C[3 * a] * dp[0] + C[3 * a + 1] * dp[1] + C[3 * a + 2] * dp[2]);
@@ -943,17 +944,17 @@ __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* 
         bP3[a] += cn * gdot * bp[a];
         bd3[a] += cn * sP * gW[a];
 #pragma unroll
-        for (int b = 0; b < 3; ++b) {
-          spd[3 * a + b] += W * bp[a] * dp[b];
-          ctb[b] += C[3 * a + b] * bp[a];
-        }
+        for (int b = 0; b < 3; ++b) spd[3 * a + b] += W * bp[a] * dp[b];
       }
 #pragma unroll
       for (int b = 0; b < 3; ++b) {
         const float hd = H[3 * b] * d3[0] + H[3 * b + 1] * d3[1] + H[3 * b + 2] * d3[2];
-        bx[b] += s * gW[b] - W * m * ctb[b] + cn * sP * hd;
+        bx[b] += s * gW[b] + cn * sP * hd;
       }
     }
+    // - sum_nodes W m C^T bp = - m C^T sp
+#pragma unroll
+    for (int b = 0; b < 3; ++b) bx[b] -= m * (C[b] * sp[0] + C[3 + b] * sp[1] + C[6 + b] * sp[2]);
     // in-plane corner forces: f1 = k P (r1 + r2), f2 = -k P r1, f3 = -k P r2
     const float kf = vol * dt;
     float bf[3][3];
