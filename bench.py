@@ -43,14 +43,14 @@ UNIT = "particle-steps/s"
 # excluded), for each kernel of the substep and its adjoint; see DESIGN.md.
 KERNEL_BYTES = {
     "k_tri_forward": {"tri": 252},
-    "k_point_p2g": {"vertex": 72, "corner": 16},
+    "k_point_p2g": {"vertex": 88},
     "k_grid": {"node": 48},
     "k_g2p": {"vertex": 84, "tri": 156},
     "k_g2p_adj": {"vertex": 96, "tri": 180},
     "k_grid_adj": {"node": 64},
-    "k_point_adj": {"vertex": 144, "corner": 16},
+    "k_point_adj": {"vertex": 156},
     "k_tri_adj": {"tri": 396},
-    "k_vertex_collect": {"vertex": 48, "corner": 28},
+    "k_vertex_collect": {"vertex": 112},
 }
 # Whole fwd+bwd substep, per particle (float32): vertex 420 B, triangle 1068 B.
 STEP_BYTES = {"vertex": 420, "tri": 1068}
