@@ -194,6 +194,12 @@ __global__ void __launch_bounds__(256, MINB) k_tri_forward(BatchDev B, const flo
   float mv[3] = {0.f, 0.f, 0.f}, A[9], cP3[3] = {0.f, 0.f, 0.f}, d3[3] = {0.f, 0.f, 0.f};
   const float m = I.m_q;
   if (valid) {
+    // the triangle's own (coalesced) loads first, so that their latency
+    // overlaps the dependent vertex gathers of load_tri
+    float dl3[3], n0[3], Di[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) A[q] = __ldg(S.t + q * nt + t) * m;
+    load_tri_rest(B, R, S, t, dl3, n0, Di);
     TriGeom g;
     load_tri(B, S, R, t, true, g);
     make_stencil(g.xc, I, st, B.status, ch.inst);
@@ -201,10 +207,6 @@ __global__ void __launch_bounds__(256, MINB) k_tri_forward(BatchDev B, const flo
     float mu, la;
     lame(prm[PRM_E], prm[PRM_NU], mu, la);
     const float ks = prm[PRM_KS], kc = prm[PRM_KC];
-    float dl3[3], n0[3], Di[9];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) A[q] = __ldg(S.t + q * nt + t) * m;
-    load_tri_rest(B, R, S, t, dl3, n0, Di);
     M3<float> d, Fe;
     tri_F(g, dl3, n0, Di, d, Fe);
     if (fdev) {  // stress from the F kept across a rest-frame reset (replay)
@@ -300,29 +302,35 @@ __global__ void __launch_bounds__(256) k_point_p2g(BatchDev B, const float* __re
   Sten st;
   float base_v[3] = {0.f, 0.f, 0.f}, A[9];
   if (valid) {
-    float X[3];
+    // every load of the particle first (one round of memory latency)
+    float X[3], vl[3] = {0.f, 0.f, 0.f};
+    float4 fs = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int a = 0; a < 3; ++a) X[a] = __ldg(x0 + a * n + p) + __ldg(arr + a * n + p);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) A[q] = m * __ldg(arr + (6 + q) * n + p);
+    if (ch.kind == CHUNK_VERTEX) {
+      fs = B.fvert[p];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) vl[a] = __ldg(arr + (3 + a) * n + p);
+    }
     make_stencil(X, I, st, B.status, ch.inst);
     if (ch.kind == CHUNK_VERTEX) {
-      const float4 fs = B.fvert[p];
       const float f[3] = {fs.x, fs.y, fs.z};
       if (fv_out) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) fv_out[a * (long long)B.nv + p] = f[a];
       }
       // temp_v = v + (0, dt*scene_scaling*g, 0) (simulation.py:182)
-      base_v[0] = m * __ldg(arr + 3 * n + p) + f[0];
-      base_v[1] = m * (__ldg(arr + 4 * n + p) + I.gravity_dv) + f[1];
-      base_v[2] = m * __ldg(arr + 5 * n + p) + f[2];
+      base_v[0] = m * vl[0] + f[0];
+      base_v[1] = m * (vl[1] + I.gravity_dv) + f[1];
+      base_v[2] = m * vl[2] + f[2];
     } else if (ch.kind == CHUNK_OPERATOR) {
       float v[3];
       long long i0, i1;
       operator_velocity(B, I, traj, step, window, p, v, i0, i1);
       base_v[0] = m * v[0]; base_v[1] = m * v[1]; base_v[2] = m * v[2];
     }  // cube: affine momentum only (simulation.py:150-152)
-#pragma unroll
-    for (int q = 0; q < 9; ++q) A[q] = m * __ldg(arr + (6 + q) * n + p);
   }
   const float dx = I.dx;
   warp_scatter<true>(B, I, ch.inst, st.base, valid, [=](int oi, int oj, int ok) -> float4 {
@@ -558,7 +566,22 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
     float X[3];
     float *ai = nullptr, *ao = nullptr, *aa = nullptr;
     long long n = 0;
+    // triangle: its own loads first, overlapping the vertex gathers
+    float Cn[9], d3[3], bd3o[3], bCo[9];
     if (tri) {
+      const long long nt = B.nt;
+      if (snext) {
+        const float* cn = snext + 15LL * B.nv;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) Cn[q] = __ldg(cn + q * nt + idx);
+      }
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        d3[q] = __ldg(R.n0 + q * nt + idx) + __ldg(Si.t + (9 + q) * nt + idx);
+        bd3o[q] = __ldg(Ao.t + (9 + q) * nt + idx);
+      }
+#pragma unroll
+      for (int q = 0; q < 9; ++q) bCo[q] = __ldg(Ao.t + q * nt + idx);
       TriGeom g;
       load_tri(B, Si, R, idx, false, g);
       X[0] = g.xc[0]; X[1] = g.xc[1]; X[2] = g.xc[2];
@@ -577,13 +600,10 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
       const long long nt = B.nt;
       const float damping = __ldg(params + ch.inst * PRM_STRIDE + PRM_DAMPING);
       const float keep = 1.f - damping;
-      float Cn[9], sym[9];
+      float sym[9];
       if (snext && keep > 0.f) {
-        // the damped C of the forward is the next state's C; its symmetric
-        // part is keep times that of the gathered C (uniform per chunk)
-        const float* cn = snext + 15LL * B.nv;
-#pragma unroll
-        for (int q = 0; q < 9; ++q) Cn[q] = __ldg(cn + q * nt + idx);
+        // the damped C of the forward is the next state's C (loaded above); its
+        // symmetric part is keep times that of the gathered C (uniform per chunk)
         const float ik = 1.f / keep;
 #pragma unroll
         for (int a = 0; a < 3; ++a)
@@ -614,14 +634,6 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
             Cn[3 * a + b] = 0.5f * (Ct[3 * a + b] - Ct[3 * b + a]) + keep * sym[3 * a + b];
           }
       }
-      float d3[3], bd3o[3], bCo[9];
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        d3[q] = __ldg(R.n0 + q * nt + idx) + __ldg(Si.t + (9 + q) * nt + idx);
-        bd3o[q] = __ldg(Ao.t + (9 + q) * nt + idx);
-      }
-#pragma unroll
-      for (int q = 0; q < 9; ++q) bCo[q] = __ldg(Ao.t + q * nt + idx);
       // M = dt C + dt^2/2 C C ; d3' = d3 + M d3
       float Mm[9];
 #pragma unroll
@@ -897,14 +909,14 @@ __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* 
   const float ks = prm[PRM_KS], kc = prm[PRM_KC];
   float gsum[4] = {0.f, 0.f, 0.f, 0.f};
   if (valid) {
+    float C[9], dl3[3], n0[3], Di[9];   // own loads first, overlapping the vertex gathers
+#pragma unroll
+    for (int q = 0; q < 9; ++q) C[q] = __ldg(Si.t + q * nt + t);
+    load_tri_rest(B, R, Si, t, dl3, n0, Di);
     TriGeom g;
     load_tri(B, Si, R, t, true, g);
     Sten st;
     make_stencil(g.xc, I, st, B.status, ch.inst);
-    float C[9], dl3[3], n0[3], Di[9];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) C[q] = __ldg(Si.t + q * nt + t);
-    load_tri_rest(B, R, Si, t, dl3, n0, Di);
     M3<float> d, Fe;
     tri_F(g, dl3, n0, Di, d, Fe);
     const float d3[3] = {d.m[2], d.m[5], d.m[8]};
