@@ -82,13 +82,13 @@ def tune(scenes: Sequence[ClothScene], dt: float, substeps: int = 3, device=None
     runs.sort(key=lambda r: r[0])
     _, chunk, mode, _ = runs[0]
     per_level = {}
-    for level in (1, 2, 3):
+    for level in (1, 2, 3, 4):
         b = ClothBatch(scenes, dt=dt, chunk=chunk, scatter_mode=mode, min_blocks=(level,) * 3, device=device)
         _time_substeps(b, 1)
         per_level[level] = _time_substeps(b, substeps)
         b.close()
         del b
-    mb = [min((1, 2, 3), key=lambda lv: per_level[lv].get(k, float("inf"))) for k in HEAVY]
+    mb = [min((1, 2, 3, 4), key=lambda lv: per_level[lv].get(k, float("inf"))) for k in HEAVY]
     cfg = {"chunk": chunk, "scatter_mode": mode, "min_blocks": mb}
     if verbose:
         for lv, t in per_level.items():

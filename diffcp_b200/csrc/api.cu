@@ -57,7 +57,7 @@ int validate(const DcpInstance* in, int n, const DcpOptions* opt) {
   if (!(opt->dt > 0.f)) return fail(DCP_ERR_INVALID, "dt must be positive");
   if (opt->scatter_mode < 0 || opt->scatter_mode > 1) return fail(DCP_ERR_INVALID, "scatter_mode must be 0 or 1");
   for (int k = 0; k < 3; ++k)
-    if (opt->min_blocks[k] < 0 || opt->min_blocks[k] > 3) return fail(DCP_ERR_INVALID, "min_blocks must be 0..3");
+    if (opt->min_blocks[k] < 0 || opt->min_blocks[k] > 4) return fail(DCP_ERR_INVALID, "min_blocks must be 0..4");
   for (int i = 0; i < n; ++i) {
     const DcpInstance& I = in[i];
     char buf[160];

@@ -1242,9 +1242,9 @@ const char* const kKernelNames[KID_COUNT] = {
 
 static inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 // Register-cap variants of the three register-heavy kernels: MINB resident
-// 256-thread CTAs per SM (1 = no cap).
+// 256-thread CTAs per SM (1 = no cap; 4 = 64 registers).
 #define DCP_MINB(kernel, L, i) \
-  (L.min_blocks[i] >= 3 ? kernel<3> : (L.min_blocks[i] == 2 ? kernel<2> : kernel<1>))
+  (L.min_blocks[i] >= 4 ? kernel<4> : L.min_blocks[i] == 3 ? kernel<3> : (L.min_blocks[i] == 2 ? kernel<2> : kernel<1>))
 #define DCP_LAUNCH(id, ...)                   \
   do {                                        \
     ProfScope _scope(L.prof, (id), s);        \
