@@ -920,11 +920,21 @@ __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* 
     M3<float> d, Fe;
     tri_F(g, dl3, n0, Di, d, Fe);
     const float d3[3] = {d.m[2], d.m[5], d.m[8]};
-    Stress<float> sts;
-    stress_forward<float>(Fe, mu, la, ks, kc, sts);
+    // The stencil loop needs only P's third column, which depends on the QR
+    // alone: P[:,2] = Q (A R^-T)[:,2] = k_s (r02 q1 + r12 q2) + A22 / n3 q3
+    // (R^-1 is upper triangular).  The full stress is formed after the loop,
+    // so that it is not held in registers across it.
+    float P3[3];
+    {
+      QR<float> q;
+      qr_forward(Fe, q);
+      const float a22 = q.a3 <= 0.f ? (-kc) * (q.a3 * q.a3) : 0.f;
+      P3[0] = ks * (q.r02 * q.q1.x + q.r12 * q.q2.x) + a22 * q.q3.x;
+      P3[1] = ks * (q.r02 * q.q1.y + q.r12 * q.q2.y) + a22 * q.q3.y;
+      P3[2] = ks * (q.r02 * q.q1.z + q.r12 * q.q2.z) + a22 * q.q3.z;
+    }
     const float vol = I.vol_q, dt = B.dt, m = I.m_q, dx = I.dx, inv_dx = I.inv_dx;
     const float cn = -vol * dt;
-    const float P3[3] = {sts.P.m[2], sts.P.m[5], sts.P.m[8]};
     float sp[3] = {0.f, 0.f, 0.f}, spd[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     float bP3[3] = {0.f, 0.f, 0.f}, bd3[3] = {0.f, 0.f, 0.f}, bx[3] = {0.f, 0.f, 0.f};
     const float mv[3] = {m * g.vc[0], m * g.vc[1], m * g.vc[2]};
@@ -967,6 +977,8 @@ __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* 
     // - sum_nodes W m C^T bp = - m C^T sp
 #pragma unroll
     for (int b = 0; b < 3; ++b) bx[b] -= m * (C[b] * sp[0] + C[3 + b] * sp[1] + C[6 + b] * sp[2]);
+    Stress<float> sts;
+    stress_forward<float>(Fe, mu, la, ks, kc, sts);
     // in-plane corner forces: f1 = k P (r1 + r2), f2 = -k P r1, f3 = -k P r2
     const float kf = vol * dt;
     float bf[3][3];
