@@ -3,8 +3,8 @@
 Chooses, by timing a few eager forward and adjoint substeps of the actual
 workload on the device:
   * ``chunk``        particles per CTA (64, 128, 256),
-  * ``scatter_mode`` warp-aggregated runs (0) or one atomic per particle and
-                     node (1),
+  * ``scatter_mode`` warp-aggregated runs (0), one atomic per particle and
+                     node (1), or lane pairs sharing a base cell (2),
   * ``min_blocks``   the register cap of each register-heavy kernel
                      (k_tri_forward, k_g2p_adj, k_tri_adj), chosen per kernel
                      from the per-kernel CUDA-event times of one run per level.
@@ -69,14 +69,15 @@ def tune(scenes: Sequence[ClothScene], dt: float, substeps: int = 3, device=None
             return table[key]["config"]
     runs = []
     for chunk in (64, 128, 256):
-        for mode in (0, 1):
+        for mode in (0, 1, 2):
             b = ClothBatch(scenes, dt=dt, chunk=chunk, scatter_mode=mode, min_blocks=DEFAULT["min_blocks"],
                            device=device)
             _time_substeps(b, 1)
             t = _time_substeps(b, substeps)
             runs.append((sum(t.values()), chunk, mode, t))
             if verbose:
-                print("chunk %3d scatter %d: %.3f ms" % (chunk, mode, sum(t.values())))
+                print("chunk %3d scatter %d: %.3f ms %s" % (chunk, mode, sum(t.values()),
+                                                           {k: round(v, 3) for k, v in sorted(t.items())}))
             b.close()
             del b
     runs.sort(key=lambda r: r[0])

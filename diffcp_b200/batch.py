@@ -54,13 +54,15 @@ class ClothBatch:
         self.vperm, self.tperm = [], []
         xv, xo, xc = [], [], []
         for i, sc in enumerate(self.scenes):
+            # Morton order of the stencil base cells (floor(x / dx - 0.5)): particles that
+            # share a base cell, and so all 27 stencil nodes, sit next to each other
             dx = 1.0 / sc.n_grid
-            vp = morton_order(sc.vertices, dx) if reorder else np.arange(sc.n_vertex)
+            vp = morton_order(sc.vertices - 0.5 * dx, dx) if reorder else np.arange(sc.n_vertex)
             inv = np.empty_like(vp)
             inv[vp] = np.arange(len(vp))
             tris = inv[np.asarray(sc.triangles)]
             cen = sc.vertices[vp][tris].mean(1)
-            tp = morton_order(cen, dx) if reorder else np.arange(sc.n_tri)
+            tp = morton_order(cen - 0.5 * dx, dx) if reorder else np.arange(sc.n_tri)
             tri_all.append(tris[tp])
             rank_all.append(vp)
             self.vperm.append(vp)

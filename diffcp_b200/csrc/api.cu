@@ -55,7 +55,7 @@ int validate(const DcpInstance* in, int n, const DcpOptions* opt) {
   if (!opt) return fail(DCP_ERR_INVALID, "options missing");
   if (opt->chunk < 32 || opt->chunk > 256 || opt->chunk % 32) return fail(DCP_ERR_INVALID, "chunk must be 32..256, multiple of 32");
   if (!(opt->dt > 0.f)) return fail(DCP_ERR_INVALID, "dt must be positive");
-  if (opt->scatter_mode < 0 || opt->scatter_mode > 1) return fail(DCP_ERR_INVALID, "scatter_mode must be 0 or 1");
+  if (opt->scatter_mode < 0 || opt->scatter_mode > 2) return fail(DCP_ERR_INVALID, "scatter_mode must be 0, 1 or 2");
   for (int k = 0; k < 3; ++k)
     if (opt->min_blocks[k] < 0 || opt->min_blocks[k] > 4) return fail(DCP_ERR_INVALID, "min_blocks must be 0..4");
   for (int i = 0; i < n; ++i) {

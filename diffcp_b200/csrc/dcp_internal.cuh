@@ -192,7 +192,7 @@ __device__ __forceinline__ void mark_block(long long node, unsigned* flags, int*
 
 // ------------------------------------------------------------ warp scatter
 // Particle-centric scatter of 27-node stencils with warp aggregation.  The
-// particles of a chunk are in Morton order at cell granularity, so particles
+// particles of a chunk are in Morton order of their base cells, so particles
 // sharing a base cell sit in consecutive lanes.  Each run of equal base cells
 // is reduced with shuffles (exact float32 sums, as many shuffle rounds as the
 // longest run needs) and only the run's first lane issues the vector atomic
@@ -205,6 +205,46 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
                                              bool valid, F&& contrib) {
   const unsigned FULL = 0xffffffffu;
   float4* grid = (MARK ? B.grid_pm : B.grid_adj) + I.node_off;
+  if (B.scatter_mode == 2) {
+    // pairs: lanes 2i and 2i+1 whose particles share a base cell (neighbours
+    // in Morton order often do) add their values with one shuffle per
+    // component and issue one atomic per node; other lanes issue their own
+    const int lane = threadIdx.x & 31;
+    const int key = valid ? ((base[0] << 22) | (base[1] << 11) | base[2]) : -1 - lane;
+    const bool pair = __shfl_xor_sync(FULL, key, 1) == key;
+    const bool issue = valid && (!pair || (lane & 1) == 0);
+    if (MARK && issue) {
+#pragma unroll
+      for (int bi = 0; bi < 2; ++bi)
+#pragma unroll
+        for (int bj = 0; bj < 2; ++bj)
+#pragma unroll
+          for (int bk = 0; bk < 2; ++bk) {
+            const int i = base[0] + 2 * bi, j = base[1] + 2 * bj, k = base[2] + 2 * bk;
+            if ((bi && (i >> 2) == (base[0] >> 2)) || (bj && (j >> 2) == (base[1] >> 2)) ||
+                (bk && (k >> 2) == (base[2] >> 2)))
+              continue;
+            mark_block(node_index(I, i, j, k), B.flags, B.list_blk, B.list_inst, B.counters, inst);
+          }
+    }
+    const NodeOffsets no = node_offsets(I, base);
+#pragma unroll
+    for (int oi = 0; oi < 3; ++oi)
+#pragma unroll
+      for (int oj = 0; oj < 3; ++oj)
+#pragma unroll
+        for (int ok = 0; ok < 3; ++ok) {
+          float4 v = valid ? contrib(oi, oj, ok) : make_float4(0.f, 0.f, 0.f, 0.f);
+          const float x = __shfl_xor_sync(FULL, v.x, 1), y = __shfl_xor_sync(FULL, v.y, 1);
+          const float z = __shfl_xor_sync(FULL, v.z, 1), w = __shfl_xor_sync(FULL, v.w, 1);
+          if (pair) {
+            v.x += x; v.y += y; v.z += z; v.w += w;
+          }
+          if (issue && (v.x != 0.f || v.y != 0.f || v.z != 0.f || v.w != 0.f))
+            atomicAdd(grid + (no.ax[oi] + no.ay[oj] + no.az[ok]), v);
+        }
+    return;
+  }
   if (B.scatter_mode == 1) {  // per-lane atomics: no shuffles, more L2 traffic
     if (!valid) return;
     if (MARK) {

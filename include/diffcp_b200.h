@@ -88,7 +88,8 @@ typedef struct DcpOptions {
   int32_t chunk;       /* particles per CTA: multiple of 32 in [32, 256] */
   int32_t svd_grad;    /* DCP_SVD_GRAD_* */
   int32_t grid_ctas;   /* CTAs of the grid-update kernels, 0 = default */
-  int32_t scatter_mode; /* 0: warp-aggregated scatter, 1: one atomic per particle and node */
+  int32_t scatter_mode; /* 0: warp-aggregated scatter, 1: one atomic per particle and node,
+                           2: lane pairs with the same base cell merged by one shuffle */
   int32_t min_blocks[3]; /* register caps of k_tri_forward, k_g2p_adj, k_tri_adj as resident 256-thread
                            CTAs per SM (1 = none, 2, 3, 4); 0 = default */
 } DcpOptions;
