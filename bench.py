@@ -211,8 +211,7 @@ def profile_substeps(args):
     scenes, info = workload(args.workload, 0)
     cache = args.tune_cache or autotune.CACHE
     launch = (autotune.cached(scenes, info["dt"], cache=cache) if os.path.exists(cache) else None) or autotune.DEFAULT
-    b = ClothBatch(scenes, dt=info["dt"], chunk=launch["chunk"], scatter_mode=launch["scatter_mode"],
-                   min_blocks=launch["min_blocks"])
+    b = ClothBatch(scenes, dt=info["dt"], **autotune.batch_kwargs(launch))
     n = args.profile_substeps
     sim = BatchSim(b, n_steps=n, ckpt_every=1, use_graph=False, tape="auto")
     for _ in range(2):
@@ -279,8 +278,7 @@ def main():
     else:
         launch = autotune.cached(scenes, info["dt"], cache=cache) if os.path.exists(cache) else None
         launch = launch or dict(autotune.DEFAULT, source="default")
-    batch = ClothBatch(scenes, dt=info["dt"], device=dev, chunk=launch["chunk"], scatter_mode=launch["scatter_mode"],
-                       min_blocks=launch["min_blocks"])
+    batch = ClothBatch(scenes, dt=info["dt"], device=dev, **autotune.batch_kwargs(launch))
     tape = None if args.no_tape else "auto"
     sim = BatchSim(batch, n_steps=info["n_steps"], ckpt_every=info["ckpt_every"], use_graph=True, tape=tape)
     params = batch.params.clone().requires_grad_(True)
@@ -394,8 +392,7 @@ def main():
     if not args.no_single and len(scenes) > 1:
         sizes = [s_.n_vertex + s_.n_tri for s_ in scenes]
         sc1 = scenes[int(np.argsort(sizes)[len(sizes) // 2])]
-        b1 = ClothBatch([sc1], dt=info["dt"], device=dev, chunk=launch["chunk"],
-                        scatter_mode=launch["scatter_mode"], min_blocks=launch["min_blocks"])
+        b1 = ClothBatch([sc1], dt=info["dt"], device=dev, **autotune.batch_kwargs(launch))
         sim1 = BatchSim(b1, n_steps=info["n_steps"], ckpt_every=info["ckpt_every"], use_graph=False, tape=tape)
         p1 = b1.params.clone().requires_grad_(True)
         t1 = b1.traj.clone().requires_grad_(True)

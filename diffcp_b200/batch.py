@@ -38,7 +38,7 @@ class ClothBatch:
 
     def __init__(self, scenes: Sequence[ClothScene], dt: float, chunk: int = 128, svd_grad: str = "exact",
                  grid_ctas: int = 0, device=None, reorder: bool = True, scatter_mode: int = 0,
-                 min_blocks: Sequence[int] = (0, 0, 0)):
+                 min_blocks: Sequence[int] = (0, 0, 0), adj_scatter_mode: Optional[int] = None):
         self.device = torch.device(device if device is not None else "cuda")
         if self.device.type != "cuda":
             raise ValueError("diffcp_b200 runs on CUDA devices only")
@@ -85,7 +85,8 @@ class ClothBatch:
             I.n_traj_steps = 0 if sc.velocities is None else int(sc.velocities.shape[0])
         self._insts = insts
         opt = DcpOptions(dt=self.dt, chunk=chunk, svd_grad=native.SVD_GRAD[svd_grad], grid_ctas=grid_ctas,
-                         scatter_mode=scatter_mode, min_blocks=(ctypes.c_int32 * 3)(*min_blocks))
+                         scatter_mode=scatter_mode, min_blocks=(ctypes.c_int32 * 3)(*min_blocks),
+                         adj_scatter_mode=scatter_mode if adj_scatter_mode is None else adj_scatter_mode)
         self._opt = opt
         sizes = DcpSizes()
         check(self.lib.dcp_plan(insts, n, ctypes.byref(opt), ctypes.byref(sizes)), "dcp_plan")

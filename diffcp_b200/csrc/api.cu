@@ -56,6 +56,8 @@ int validate(const DcpInstance* in, int n, const DcpOptions* opt) {
   if (opt->chunk < 32 || opt->chunk > 256 || opt->chunk % 32) return fail(DCP_ERR_INVALID, "chunk must be 32..256, multiple of 32");
   if (!(opt->dt > 0.f)) return fail(DCP_ERR_INVALID, "dt must be positive");
   if (opt->scatter_mode < 0 || opt->scatter_mode > 2) return fail(DCP_ERR_INVALID, "scatter_mode must be 0, 1 or 2");
+  if (opt->adj_scatter_mode < 0 || opt->adj_scatter_mode > 2)
+    return fail(DCP_ERR_INVALID, "adj_scatter_mode must be 0, 1 or 2");
   for (int k = 0; k < 3; ++k)
     if (opt->min_blocks[k] < 0 || opt->min_blocks[k] > 4) return fail(DCP_ERR_INVALID, "min_blocks must be 0..4");
   for (int i = 0; i < n; ++i) {
@@ -261,6 +263,7 @@ int dcp_create(const DcpInstance* inst, int32_t n_inst, const DcpOptions* opt, c
   B.dt = opt->dt;
   B.svd_grad = opt->svd_grad;
   B.scatter_mode = opt->scatter_mode;
+  B.adj_scatter_mode = opt->adj_scatter_mode;
   B.grid_pm = (float4*)(wd + L.off_pm);
   B.grid_v = (float4*)(wd + L.off_v);
   B.grid_adj = (float4*)(wd + L.off_adj);

@@ -58,7 +58,8 @@ struct BatchDev {
   const int* vertex_rank;  // [nv] tie-break rank for the Chamfer argmin
   float dt;
   int svd_grad;
-  int scatter_mode;  // 0: warp-aggregated runs, 1: one atomic per lane and node
+  int scatter_mode;      // P2G kernels: 0 warp-aggregated runs, 1 one atomic per lane and node, 2 lane pairs
+  int adj_scatter_mode;  // k_g2p_adj, same values
   // workspace
   float4* grid_pm;
   float4* grid_v;
@@ -205,7 +206,8 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
                                              bool valid, F&& contrib) {
   const unsigned FULL = 0xffffffffu;
   float4* grid = (MARK ? B.grid_pm : B.grid_adj) + I.node_off;
-  if (B.scatter_mode == 2) {
+  const int mode = MARK ? B.scatter_mode : B.adj_scatter_mode;
+  if (mode == 2) {
     // pairs: lanes 2i and 2i+1 whose particles share a base cell (neighbours
     // in Morton order often do) add their values with one shuffle per
     // component and issue one atomic per node; other lanes issue their own
@@ -245,7 +247,7 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
         }
     return;
   }
-  if (B.scatter_mode == 1) {  // per-lane atomics: no shuffles, more L2 traffic
+  if (mode == 1) {  // per-lane atomics: no shuffles, more L2 traffic
     if (!valid) return;
     if (MARK) {
 #pragma unroll

@@ -45,7 +45,8 @@ class DcpInstance(ctypes.Structure):
 
 class DcpOptions(ctypes.Structure):
     _fields_ = [("dt", c_float), ("chunk", c_int32), ("svd_grad", c_int32), ("grid_ctas", c_int32),
-                ("scatter_mode", c_int32), ("min_blocks", c_int32 * 3)]
+                ("scatter_mode", c_int32), ("min_blocks", c_int32 * 3),
+                ("adj_scatter_mode", c_int32)]
 
 
 class DcpSizes(ctypes.Structure):

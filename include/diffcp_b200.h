@@ -92,6 +92,8 @@ typedef struct DcpOptions {
                            2: lane pairs with the same base cell merged by one shuffle */
   int32_t min_blocks[3]; /* register caps of k_tri_forward, k_g2p_adj, k_tri_adj as resident 256-thread
                            CTAs per SM (1 = none, 2, 3, 4); 0 = default */
+  int32_t adj_scatter_mode; /* scatter of the adjoint G2P kernel (k_g2p_adj), same values as
+                               scatter_mode, which covers the two P2G kernels */
 } DcpOptions;
 
 typedef struct DcpSizes {

@@ -273,14 +273,15 @@ def test_chunk_size_does_not_change_results(chunk):
     np.testing.assert_allclose(t1, t2, rtol=ORDER_RTOL, atol=ORDER_RTOL * np.abs(t1).max())
 
 
-@pytest.mark.parametrize("mode", [1, 2])
-def test_scatter_modes_give_the_same_results(mode):
-    """Warp-aggregated runs (scatter_mode 0), per-lane atomics (1) and lane
-    pairs (2) sum the same contributions."""
+@pytest.mark.parametrize("mode,adj_mode", [(1, 1), (2, 2), (2, 1), (0, 2)])
+def test_scatter_modes_give_the_same_results(mode, adj_mode):
+    """Warp-aggregated runs (scatter mode 0), per-lane atomics (1) and lane
+    pairs (2), in the P2G kernels and the adjoint G2P kernel independently,
+    sum the same contributions."""
     n = 12
     sc = small_sheet(n=9, n_steps=n)
     l0, g0, t0, _ = _sheet_grads(sc, n, scatter_mode=0)
-    l1, g1, t1, _ = _sheet_grads(sc, n, scatter_mode=mode)
+    l1, g1, t1, _ = _sheet_grads(sc, n, scatter_mode=mode, adj_scatter_mode=adj_mode)
     assert float(l1[0]) == pytest.approx(float(l0[0]), rel=1e-6)
     np.testing.assert_allclose(g1, g0, rtol=ORDER_RTOL, atol=1e-16)
     np.testing.assert_allclose(t1, t0, rtol=ORDER_RTOL, atol=ORDER_RTOL * np.abs(t0).max())

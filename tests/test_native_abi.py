@@ -65,6 +65,9 @@ def test_plan_sizes_and_validation():
     bad = native.DcpOptions(dt=1e-4, chunk=100, svd_grad=0, grid_ctas=0)
     assert L.dcp_plan(insts, 2, ctypes.byref(bad), ctypes.byref(s)) == 1
     assert b"chunk" in L.dcp_last_error()
+    bad = native.DcpOptions(dt=1e-4, chunk=128, svd_grad=0, grid_ctas=0, adj_scatter_mode=3)
+    assert L.dcp_plan(insts, 2, ctypes.byref(bad), ctypes.byref(s)) == 1
+    assert b"adj_scatter_mode" in L.dcp_last_error()
     insts2 = (native.DcpInstance * 1)(_inst(gripper_mode=1, n_grippers=2, group_size=3, n_operator=5, n_actions=4,
                                             keyframe_interval=0.03))
     assert L.dcp_plan(insts2, 1, ctypes.byref(opt), ctypes.byref(s)) == 1
