@@ -20,6 +20,10 @@ LIB = os.path.join(LIB_DIR, "libdiffcp_b200.so")
 SOURCES = ["kernels.cu", "api.cu", "chamfer_static.cu"]
 HEADERS = ["cloth_math.cuh", "dcp_internal.cuh", "dcp_launch.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# The substep kernels divide and take square roots with the approximate forms
+# (about 2 ulp); the Chamfer kernels, whose minimum and tie-break follow the
+# reference's float32 rounding, use explicitly rounded operations throughout.
+EXTRA = {"kernels.cu": ["-prec-div=false", "-prec-sqrt=false"]}
 
 
 def nvcc() -> str:
@@ -44,7 +48,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     objs = []
     for src in SOURCES:
         obj = os.path.join(LIB_DIR, src.replace(".cu", ".o"))
-        cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-c",
+        cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", *EXTRA.get(src, []), "-Xcompiler", "-fPIC", "-c",
                os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")

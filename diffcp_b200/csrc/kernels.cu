@@ -270,14 +270,14 @@ __device__ __forceinline__ const float* point_rest(const RestP& R, int kind) {
 __device__ __forceinline__ bool operator_velocity(const BatchDev& B, const InstDev& I, const float* traj, int step,
                                                   int window, long long p, float v[3], long long& i0, long long& i1) {
   const float tt = (float)step * B.dt;
-  const int frame = (int)(tt / I.interval) + I.frames_per_window * window;
+  const int frame = (int)__fdiv_rn(tt, I.interval) + I.frames_per_window * window;
   const int gid = (int)((p - I.o_off) / I.group_size);
   v[0] = v[1] = v[2] = 0.f;
   if (frame + 1 < I.n_actions && frame >= 0) {
     i0 = I.traj_off + ((long long)frame * I.n_grip + gid) * 3;
     i1 = I.traj_off + ((long long)(frame + 1) * I.n_grip + gid) * 3;
 #pragma unroll
-    for (int a = 0; a < 3; ++a) v[a] = (__ldg(traj + i1 + a) - __ldg(traj + i0 + a)) / I.interval;
+    for (int a = 0; a < 3; ++a) v[a] = __fdiv_rn(__ldg(traj + i1 + a) - __ldg(traj + i0 + a), I.interval);
     return true;
   }
   return false;
@@ -935,48 +935,88 @@ __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* 
     }
     const float vol = I.vol_q, dt = B.dt, m = I.m_q, dx = I.dx, inv_dx = I.inv_dx;
     const float cn = -vol * dt;
-    float sp[3] = {0.f, 0.f, 0.f}, spd[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    float bP3[3] = {0.f, 0.f, 0.f}, bd3[3] = {0.f, 0.f, 0.f}, bx[3] = {0.f, 0.f, 0.f};
-    const float mv[3] = {m * g.vc[0], m * g.vc[1], m * g.vc[2]};
     const float i2 = inv_dx * inv_dx;
+    // Per-node factors are products of per-axis ones: slopes pre-scaled by
+    // 1/dx, curvatures (1, -2, 1) by 1/dx^2.  The APIC payload
+    // m (v + C dpos), dpos = (o - fx) dx, is K + Cm o with Cm = m dx C and
+    // K = m v - Cm fx, so each node adds the per-axis terms of its offsets o
+    // (0, 1 or 2) instead of forming C dpos.  Sums that are linear in the
+    // node's own data are accumulated as moments and finished after the loop:
+    //   mo[a][b] = sum W g_a o_b          -> sum W g_a dpos_b = dx (mo - fx_b sp_a)
+    //   hs[bc]   = sum (g . P3) H_bc      -> sum (g . P3) (H d3)_b = sum_c hs[bc] d3_c
+    float ed[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int o = 0; o < 3; ++o) ed[a][o] = st.dw[a][o] * inv_dx;
+    const float ddc[3] = {i2, -2.f * i2, i2};
+    float Cm[9], K[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+      for (int b = 0; b < 3; ++b) Cm[3 * a + b] = (m * dx) * C[3 * a + b];
+      K[a] = m * g.vc[a] - (Cm[3 * a] * st.fx[0] + Cm[3 * a + 1] * st.fx[1] + Cm[3 * a + 2] * st.fx[2]);
+    }
+    float sp[3] = {0.f, 0.f, 0.f}, mo[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float g3[3] = {0.f, 0.f, 0.f}, sg[3] = {0.f, 0.f, 0.f}, bx[3] = {0.f, 0.f, 0.f};
+    float hs[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // (00, 01, 02, 11, 12, 22)
     const float4* gnb = B.grid_adj + I.node_off;
     const NodeOffsets nofs = node_offsets(I, st.base);
 #pragma unroll
-    for (int q = 0; q < 27; ++q) {
-      const int oi = q / 9, oj = (q / 3) % 3, ok = q % 3;
-      const float w0 = st.w[0][oi], w1 = st.w[1][oj], w2 = st.w[2][ok];
-      const float e0 = st.dw[0][oi], e1 = st.dw[1][oj], e2 = st.dw[2][ok];
-      const float W = w0 * w1 * w2;
-      const float gW[3] = {e0 * w1 * w2 * inv_dx, w0 * e1 * w2 * inv_dx, w0 * w1 * e2 * inv_dx};
-      const float dd0 = bspline_dd<float>(oi), dd1 = bspline_dd<float>(oj), dd2 = bspline_dd<float>(ok);
-      const float H[9] = {dd0 * w1 * w2 * i2, e0 * e1 * w2 * i2, e0 * w1 * e2 * i2,
-                          e0 * e1 * w2 * i2, w0 * dd1 * w2 * i2, w0 * e1 * e2 * i2,
-                          e0 * w1 * e2 * i2, w0 * e1 * e2 * i2, w0 * w1 * dd2 * i2};
-      const float dp[3] = {((float)oi - st.fx[0]) * dx, ((float)oj - st.fx[1]) * dx, ((float)ok - st.fx[2]) * dx};
-      const float4 ga = __ldg(gnb + (nofs.ax[oi] + nofs.ay[oj] + nofs.az[ok]));
-      const float bp[3] = {ga.x, ga.y, ga.z};
-      const float gdot = gW[0] * d3[0] + gW[1] * d3[1] + gW[2] * d3[2];
-      const float sP = bp[0] * P3[0] + bp[1] * P3[1] + bp[2] * P3[2];
-      float s = ga.w * m;
+    for (int oi = 0; oi < 3; ++oi)
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const float pay = mv[a] + m * (C[3 * a] * dp[0] + C[3 * a + 1] * dp[1] + C[3 * a + 2] * dp[2]);
-        s += bp[a] * pay;
-        sp[a] += W * bp[a];
-        bP3[a] += cn * gdot * bp[a];
-        bd3[a] += cn * sP * gW[a];
+      for (int oj = 0; oj < 3; ++oj) {
+        const float w0 = st.w[0][oi], w1 = st.w[1][oj], e0 = ed[0][oi], e1 = ed[1][oj];
+        const float w01 = w0 * w1, e0w1 = e0 * w1, w0e1 = w0 * e1, e0e1 = e0 * e1;
+        const float d0w1 = ddc[oi] * w1, w0d1 = w0 * ddc[oj];
+        float kij[3];
 #pragma unroll
-        for (int b = 0; b < 3; ++b) spd[3 * a + b] += W * bp[a] * dp[b];
+        for (int a = 0; a < 3; ++a) kij[a] = K[a] + (float)oi * Cm[3 * a] + (float)oj * Cm[3 * a + 1];
+#pragma unroll
+        for (int ok = 0; ok < 3; ++ok) {
+          const float w2 = st.w[2][ok], e2 = ed[2][ok];
+          const float W = w01 * w2;
+          const float gW[3] = {e0w1 * w2, w0e1 * w2, w01 * e2};
+          const float H[6] = {d0w1 * w2, e0e1 * w2, e0w1 * e2, w0d1 * w2, w0e1 * e2, w01 * ddc[ok]};
+          const float4 ga = __ldg(gnb + (nofs.ax[oi] + nofs.ay[oj] + nofs.az[ok]));
+          const float bp[3] = {ga.x, ga.y, ga.z};
+          const float gdot = gW[0] * d3[0] + gW[1] * d3[1] + gW[2] * d3[2];
+          const float sP = bp[0] * P3[0] + bp[1] * P3[1] + bp[2] * P3[2];
+          float s = ga.w * m;
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            s += bp[a] * (kij[a] + (float)ok * Cm[3 * a + 2]);
+            const float Wb = W * bp[a];
+            sp[a] += Wb;
+            if (oi) mo[3 * a] += (float)oi * Wb;
+            if (oj) mo[3 * a + 1] += (float)oj * Wb;
+            if (ok) mo[3 * a + 2] += (float)ok * Wb;
+            g3[a] += gdot * bp[a];
+            sg[a] += sP * gW[a];
+          }
+#pragma unroll
+          for (int b = 0; b < 3; ++b) bx[b] += s * gW[b];
+#pragma unroll
+          for (int q = 0; q < 6; ++q) hs[q] += sP * H[q];
+        }
       }
+    float spd[9], bP3[3], bd3[3];
 #pragma unroll
-      for (int b = 0; b < 3; ++b) {
-        const float hd = H[3 * b] * d3[0] + H[3 * b + 1] * d3[1] + H[3 * b + 2] * d3[2];
-        bx[b] += s * gW[b] + cn * sP * hd;
-      }
+    for (int a = 0; a < 3; ++a) {
+      bP3[a] = cn * g3[a];
+      bd3[a] = cn * sg[a];
+#pragma unroll
+      for (int b = 0; b < 3; ++b) spd[3 * a + b] = dx * (mo[3 * a + b] - st.fx[b] * sp[a]);
     }
-    // - sum_nodes W m C^T bp = - m C^T sp
+    {
+      const float hd[3] = {hs[0] * d3[0] + hs[1] * d3[1] + hs[2] * d3[2],
+                           hs[1] * d3[0] + hs[3] * d3[1] + hs[4] * d3[2],
+                           hs[2] * d3[0] + hs[4] * d3[1] + hs[5] * d3[2]};
+      // - sum_nodes W m C^T bp = - m C^T sp = - Cm^T sp / dx
 #pragma unroll
-    for (int b = 0; b < 3; ++b) bx[b] -= m * (C[b] * sp[0] + C[3 + b] * sp[1] + C[6 + b] * sp[2]);
+      for (int b = 0; b < 3; ++b)
+        bx[b] += cn * hd[b] - inv_dx * (Cm[b] * sp[0] + Cm[3 + b] * sp[1] + Cm[6 + b] * sp[2]);
+    }
     Stress<float> sts;
     stress_forward<float>(Fe, mu, la, ks, kc, sts);
     // in-plane corner forces: f1 = k P (r1 + r2), f2 = -k P r1, f3 = -k P r2
@@ -1133,7 +1173,7 @@ __global__ void k_chamfer_loss(BatchDev B, float* __restrict__ loss) {
   __shared__ double red[32];
   const InstDev& I = B.inst[blockIdx.x];
   double s = 0.0;
-  for (int q = threadIdx.x; q < I.nq; q += blockDim.x) s += (double)(B.qmin[I.q_off + q] / (float)I.nq);
+  for (int q = threadIdx.x; q < I.nq; q += blockDim.x) s += (double)__fdiv_rn(B.qmin[I.q_off + q], (float)I.nq);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
@@ -1157,7 +1197,7 @@ __global__ void k_chamfer_bwd(BatchDev B, const float* __restrict__ rest, const 
   const long long gq = (long long)I.q_off + q;
   const int v = qarg[gq];
   if (v < 0) return;
-  const float s = __ldg(gloss + inst) / (float)I.nq * (2.f / 3.f);
+  const float s = __fdiv_rn(__ldg(gloss + inst), (float)I.nq) * (2.f / 3.f);
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const float d = (__ldg(R.xv + a * nv + v) - __ldg(targets + a * nq + gq)) + __ldg(state + a * nv + v);
