@@ -179,6 +179,13 @@ __device__ __forceinline__ void make_stencil(const float p[3], const InstDev& I,
   if (bad) atomicOr(status + inst, STATUS_OUT_OF_DOMAIN);
 }
 
+// acc + o c for a stencil offset o in {0, 1, 2}.  With o known at compile
+// time (unrolled stencil loops) this is nothing, one add or one multiply-add:
+// 0 * c cannot be folded away under IEEE rules, so o = 0 must not multiply.
+__device__ __forceinline__ float add_off(float acc, int o, float c) {
+  return o == 0 ? acc : (o == 1 ? acc + c : fmaf(2.f, c, acc));
+}
+
 __device__ __forceinline__ void mark_block(long long node, unsigned* flags, int* list_blk, int* list_inst, int* counter,
                                            int inst) {
   const long long b = node >> 6;

@@ -191,9 +191,15 @@ __global__ void __launch_bounds__(256, MINB) k_tri_forward(BatchDev B, const flo
   StateP S = state_ptrs(const_cast<float*>(sin), B.nv, B.nt, B.no);
   const RestP R = rest_ptrs(rest, B.nv, B.nt, B.no);
   Sten st;
-  float mv[3] = {0.f, 0.f, 0.f}, A[9], cP3[3] = {0.f, 0.f, 0.f}, d3[3] = {0.f, 0.f, 0.f};
+  // scatter factors: ed = slope / dx * d3 per axis, so that the normal-force
+  // weight grad W . d3 is formed from per-axis products; the APIC payload
+  // m (v + C dpos), dpos = (o - fx) dx, is K + Ad o with Ad = m dx C and
+  // K = m v - Ad fx (per-axis terms added for the node's offsets o)
+  float K[3] = {0.f, 0.f, 0.f}, Ad[9], cP3[3] = {0.f, 0.f, 0.f}, ed[3][3];
   const float m = I.m_q;
+  const float dx = I.dx, inv_dx = I.inv_dx;
   if (valid) {
+    float A[9];
     // the triangle's own (coalesced) loads first, so that their latency
     // overlaps the dependent vertex gathers of load_tri
     float dl3[3], n0[3], Di[9];
@@ -233,25 +239,25 @@ __global__ void __launch_bounds__(256, MINB) k_tri_forward(BatchDev B, const flo
     const float cn = -vol * dt;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      mv[a] = m * g.vc[a];
       cP3[a] = cn * P.m[3 * a + 2];
-      d3[a] = d.m[3 * a + 2];
+      const float ea = inv_dx * d.m[3 * a + 2];
+#pragma unroll
+      for (int o = 0; o < 3; ++o) ed[a][o] = st.dw[a][o] * ea;
+#pragma unroll
+      for (int b = 0; b < 3; ++b) Ad[3 * a + b] = dx * A[3 * a + b];
+      K[a] = m * g.vc[a] - (Ad[3 * a] * st.fx[0] + Ad[3 * a + 1] * st.fx[1] + Ad[3 * a + 2] * st.fx[2]);
     }
   }
-  const float dx = I.dx, inv_dx = I.inv_dx;
   // own-node APIC momentum, mass and normal force (simulation.py:250-265)
   warp_scatter<true>(B, I, ch.inst, st.base, valid, [=](int oi, int oj, int ok) -> float4 {
     const float w0 = st.w[0][oi], w1 = st.w[1][oj], w2 = st.w[2][ok];
-    const float W = w0 * w1 * w2;
-    const float gx = st.dw[0][oi] * inv_dx * w1 * w2;
-    const float gy = w0 * (st.dw[1][oj] * inv_dx) * w2;
-    const float gz = w0 * w1 * (st.dw[2][ok] * inv_dx);
-    const float px = ((float)oi - st.fx[0]) * dx, py = ((float)oj - st.fx[1]) * dx, pz = ((float)ok - st.fx[2]) * dx;
-    const float nrm = gx * d3[0] + gy * d3[1] + gz * d3[2];
+    const float w01 = w0 * w1;
+    const float W = w01 * w2;
+    const float nrm = (ed[0][oi] * w1 + w0 * ed[1][oj]) * w2 + w01 * ed[2][ok];
     float4 val;
-    val.x = W * (mv[0] + (A[0] * px + A[1] * py + A[2] * pz)) + nrm * cP3[0];
-    val.y = W * (mv[1] + (A[3] * px + A[4] * py + A[5] * pz)) + nrm * cP3[1];
-    val.z = W * (mv[2] + (A[6] * px + A[7] * py + A[8] * pz)) + nrm * cP3[2];
+    val.x = W * add_off(add_off(add_off(K[0], oi, Ad[0]), oj, Ad[1]), ok, Ad[2]) + nrm * cP3[0];
+    val.y = W * add_off(add_off(add_off(K[1], oi, Ad[3]), oj, Ad[4]), ok, Ad[5]) + nrm * cP3[1];
+    val.z = W * add_off(add_off(add_off(K[2], oi, Ad[6]), oj, Ad[7]), ok, Ad[8]) + nrm * cP3[2];
     val.w = W * m;
     return val;
   });
@@ -300,7 +306,9 @@ __global__ void __launch_bounds__(256) k_point_p2g(BatchDev B, const float* __re
   const float* x0 = point_rest(rest_ptrs(rest, B.nv, B.nt, B.no), ch.kind);
   const float m = ch.kind == CHUNK_VERTEX ? I.m_v : (ch.kind == CHUNK_OPERATOR ? I.m_o : I.m_c);
   Sten st;
-  float base_v[3] = {0.f, 0.f, 0.f}, A[9];
+  // payload m (v + C dpos) = K + Ad o per node (as in k_tri_forward)
+  float base_v[3] = {0.f, 0.f, 0.f}, A[9], K[3] = {0.f, 0.f, 0.f};
+  const float dx = I.dx;
   if (valid) {
     // every load of the particle first (one round of memory latency)
     float X[3], vl[3] = {0.f, 0.f, 0.f};
@@ -331,15 +339,19 @@ __global__ void __launch_bounds__(256) k_point_p2g(BatchDev B, const float* __re
       operator_velocity(B, I, traj, step, window, p, v, i0, i1);
       base_v[0] = m * v[0]; base_v[1] = m * v[1]; base_v[2] = m * v[2];
     }  // cube: affine momentum only (simulation.py:150-152)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+      for (int b = 0; b < 3; ++b) A[3 * a + b] *= dx;
+      K[a] = base_v[a] - (A[3 * a] * st.fx[0] + A[3 * a + 1] * st.fx[1] + A[3 * a + 2] * st.fx[2]);
+    }
   }
-  const float dx = I.dx;
   warp_scatter<true>(B, I, ch.inst, st.base, valid, [=](int oi, int oj, int ok) -> float4 {
-    const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
-    const float px = ((float)oi - st.fx[0]) * dx, py = ((float)oj - st.fx[1]) * dx, pz = ((float)ok - st.fx[2]) * dx;
+    const float W = (st.w[0][oi] * st.w[1][oj]) * st.w[2][ok];
     float4 val;
-    val.x = W * (base_v[0] + (A[0] * px + A[1] * py + A[2] * pz));
-    val.y = W * (base_v[1] + (A[3] * px + A[4] * py + A[5] * pz));
-    val.z = W * (base_v[2] + (A[6] * px + A[7] * py + A[8] * pz));
+    val.x = W * add_off(add_off(add_off(K[0], oi, A[0]), oj, A[1]), ok, A[2]);
+    val.y = W * add_off(add_off(add_off(K[1], oi, A[3]), oj, A[4]), ok, A[5]);
+    val.z = W * add_off(add_off(add_off(K[2], oi, A[6]), oj, A[7]), ok, A[8]);
     val.w = W * m;
     return val;
   });
@@ -417,6 +429,43 @@ __device__ __forceinline__ float3 gv_at(const float4* g, const NodeOffsets& o, i
   return make_float3(v.x, v.y, v.z);
 }
 
+// APIC gather of the grid velocities over a particle's stencil: v = sum W g
+// and C = 4/dx sum W g (x) (o - fx), the latter from the moments
+// mo[a][b] = sum W g_a o_b as C = 4/dx (mo - v fx^T) (o the node's offset
+// 0, 1, 2 per axis).  v may be null.
+__device__ __forceinline__ void gather_affine(const float4* gnb, const InstDev& I, const Sten& st, float inv_dx,
+                                              float* v_out, float C[9]) {
+  float v[3] = {0.f, 0.f, 0.f}, mo[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  const NodeOffsets nofs = node_offsets(I, st.base);
+#pragma unroll
+  for (int oi = 0; oi < 3; ++oi)
+#pragma unroll
+    for (int oj = 0; oj < 3; ++oj) {
+      const float w01 = st.w[0][oi] * st.w[1][oj];
+#pragma unroll
+      for (int ok = 0; ok < 3; ++ok) {
+        const float W = w01 * st.w[2][ok];
+        const float3 gn = gv_at(gnb, nofs, oi, oj, ok);
+        const float ga[3] = {gn.x, gn.y, gn.z};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const float Wg = W * ga[a];
+          v[a] += Wg;
+          mo[3 * a] = add_off(mo[3 * a], oi, Wg);
+          mo[3 * a + 1] = add_off(mo[3 * a + 1], oj, Wg);
+          mo[3 * a + 2] = add_off(mo[3 * a + 2], ok, Wg);
+        }
+      }
+    }
+  const float c4 = 4.f * inv_dx;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+#pragma unroll
+    for (int b = 0; b < 3; ++b) C[3 * a + b] = c4 * (mo[3 * a + b] - v[a] * st.fx[b]);
+    if (v_out) v_out[a] = v[a];
+  }
+}
+
 // TRI: launched over the triangle chunks; otherwise over the point chunks
 // (vertex, operator, cube), which follow the triangle chunks in the table.
 template <bool TRI>
@@ -436,25 +485,8 @@ __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict
     load_tri(B, Si, R, t, false, g);
     Sten st;
     make_stencil(g.xc, I, st, B.status, ch.inst);
-    float Ct[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    const float4* gnb = B.grid_v + I.node_off;
-    const NodeOffsets nofs = node_offsets(I, st.base);
-#pragma unroll
-    for (int oi = 0; oi < 3; ++oi)
-#pragma unroll
-      for (int oj = 0; oj < 3; ++oj)
-#pragma unroll
-        for (int ok = 0; ok < 3; ++ok) {
-          const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
-          const float3 gn = gv_at(gnb, nofs, oi, oj, ok);
-          const float dp[3] = {(float)oi - st.fx[0], (float)oj - st.fx[1], (float)ok - st.fx[2]};
-          const float s = 4.f * W * inv_dx;
-          const float ga[3] = {gn.x, gn.y, gn.z};
-#pragma unroll
-          for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int b = 0; b < 3; ++b) Ct[3 * a + b] += s * ga[a] * dp[b];
-        }
+    float Ct[9];
+    gather_affine(B.grid_v + I.node_off, I, st, inv_dx, nullptr, Ct);
     // C = skew + (1 - damping) sym (simulation.py:381-383)
     const float keep = 1.f - __ldg(params + ch.inst * PRM_STRIDE + PRM_DAMPING);
     float Cn[9];
@@ -506,27 +538,8 @@ __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict
   }
   Sten st;
   make_stencil(X, I, st, B.status, ch.inst);
-  float v[3] = {0.f, 0.f, 0.f}, C[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  const float4* gnb = B.grid_v + I.node_off;
-  const NodeOffsets nofs = node_offsets(I, st.base);
-#pragma unroll
-  for (int oi = 0; oi < 3; ++oi)
-#pragma unroll
-    for (int oj = 0; oj < 3; ++oj)
-#pragma unroll
-      for (int ok = 0; ok < 3; ++ok) {
-        const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
-        const float3 gn = gv_at(gnb, nofs, oi, oj, ok);
-        const float dp[3] = {(float)oi - st.fx[0], (float)oj - st.fx[1], (float)ok - st.fx[2]};
-        const float ga[3] = {gn.x, gn.y, gn.z};
-        const float s = 4.f * W * inv_dx;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          v[a] += W * ga[a];
-#pragma unroll
-          for (int b = 0; b < 3; ++b) C[3 * a + b] += s * ga[a] * dp[b];
-        }
-      }
+  float v[3], C[9];
+  gather_affine(B.grid_v + I.node_off, I, st, inv_dx, v, C);
   bool finite = true;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
@@ -561,7 +574,7 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
   const long long idx = ch.start + tid;
   Sten st;
   float gdamp[1] = {0.f};
-  float bV[3] = {0.f, 0.f, 0.f}, cbC[9];  // dL/dv' and 4 inv_dx dL/dC of the gather
+  float bV[3] = {0.f, 0.f, 0.f}, cbC[9], Kg[3] = {0.f, 0.f, 0.f};  // dL/dv', 4/dx dL/dC, node weight base
   if (valid) {
     float X[3];
     float *ai = nullptr, *ao = nullptr, *aa = nullptr;
@@ -610,22 +623,8 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
 #pragma unroll
           for (int b = 0; b < 3; ++b) sym[3 * a + b] = 0.5f * (Cn[3 * a + b] + Cn[3 * b + a]) * ik;
       } else {
-        float Ct[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        const float4* gnb = B.grid_v + I.node_off;
-        const NodeOffsets nofs = node_offsets(I, st.base);
-#pragma unroll
-        for (int q = 0; q < 27; ++q) {
-          const int oi = q / 9, oj = (q / 3) % 3, ok = q % 3;
-          const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
-          const float dp[3] = {(float)oi - st.fx[0], (float)oj - st.fx[1], (float)ok - st.fx[2]};
-          const float3 gn = gv_at(gnb, nofs, oi, oj, ok);
-          const float ga[3] = {gn.x, gn.y, gn.z};
-          const float s = 4.f * W * inv_dx;
-#pragma unroll
-          for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int b = 0; b < 3; ++b) Ct[3 * a + b] += s * ga[a] * dp[b];
-        }
+        float Ct[9];
+        gather_affine(B.grid_v + I.node_off, I, st, inv_dx, nullptr, Ct);
 #pragma unroll
         for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -689,32 +688,53 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
 #pragma unroll
       for (int q = 0; q < 9; ++q) bC[q] = __ldg(ao + (6 + q) * n + idx);
     }
-    // position adjoint of the gather (second pass over the stencil)
+    // position adjoint of the gather (second pass over the stencil).  The
+    // node's weight dL/dv' + 4/dx dL/dC (o - fx) is Kg + cbC o with
+    // cbC = 4/dx dL/dC and Kg = dL/dv' - cbC fx (per-axis terms added for the
+    // node's offsets o); the scatter below uses the same weights.
     float px[3] = {0.f, 0.f, 0.f}, vs[3] = {0.f, 0.f, 0.f};
     const float c4 = 4.f * inv_dx;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) cbC[q] = c4 * bC[q];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+      Kg[a] = bV[a] - (cbC[3 * a] * st.fx[0] + cbC[3 * a + 1] * st.fx[1] + cbC[3 * a + 2] * st.fx[2]);
+    float ed[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int o = 0; o < 3; ++o) ed[a][o] = st.dw[a][o] * inv_dx;
     const float4* gnb = B.grid_v + I.node_off;
     const NodeOffsets nofs = node_offsets(I, st.base);
 #pragma unroll
-    for (int q = 0; q < 27; ++q) {
-      const int oi = q / 9, oj = (q / 3) % 3, ok = q % 3;
-      const float w0 = st.w[0][oi], w1 = st.w[1][oj], w2 = st.w[2][ok];
-      const float W = w0 * w1 * w2;
-      const float gW[3] = {st.dw[0][oi] * w1 * w2 * inv_dx, w0 * st.dw[1][oj] * w2 * inv_dx, w0 * w1 * st.dw[2][ok] * inv_dx};
-      const float dp[3] = {(float)oi - st.fx[0], (float)oj - st.fx[1], (float)ok - st.fx[2]};
-      const float3 gn = gv_at(gnb, nofs, oi, oj, ok);
-      const float ga[3] = {gn.x, gn.y, gn.z};
-      float s1 = bV[0] * ga[0] + bV[1] * ga[1] + bV[2] * ga[2];
+    for (int oi = 0; oi < 3; ++oi)
 #pragma unroll
-      for (int a = 0; a < 3; ++a) s1 += c4 * ga[a] * (bC[3 * a] * dp[0] + bC[3 * a + 1] * dp[1] + bC[3 * a + 2] * dp[2]);
+      for (int oj = 0; oj < 3; ++oj) {
+        const float w0 = st.w[0][oi], w1 = st.w[1][oj];
+        const float w01 = w0 * w1, e0w1 = ed[0][oi] * w1, w0e1 = w0 * ed[1][oj];
+        float kij[3];
 #pragma unroll
-      for (int b = 0; b < 3; ++b) {
-        px[b] += s1 * gW[b];
-        vs[b] += W * ga[b];
+        for (int a = 0; a < 3; ++a) kij[a] = add_off(add_off(Kg[a], oi, cbC[3 * a]), oj, cbC[3 * a + 1]);
+#pragma unroll
+        for (int ok = 0; ok < 3; ++ok) {
+          const float w2 = st.w[2][ok];
+          const float W = w01 * w2;
+          const float gW[3] = {e0w1 * w2, w0e1 * w2, w01 * ed[2][ok]};
+          const float3 gn = gv_at(gnb, nofs, oi, oj, ok);
+          const float ga[3] = {gn.x, gn.y, gn.z};
+          float s1 = 0.f;
+#pragma unroll
+          for (int a = 0; a < 3; ++a) s1 += ga[a] * add_off(kij[a], ok, cbC[3 * a + 2]);
+#pragma unroll
+          for (int b = 0; b < 3; ++b) {
+            px[b] += s1 * gW[b];
+            vs[b] += W * ga[b];
+          }
+        }
       }
-    }
-    // - c4 inv_dx sum_nodes W bC^T g = - c4 inv_dx bC^T (sum_nodes W g)
+    // - c4 inv_dx sum_nodes W bC^T g = - inv_dx cbC^T (sum_nodes W g)
 #pragma unroll
-    for (int b = 0; b < 3; ++b) px[b] -= c4 * inv_dx * (bC[b] * vs[0] + bC[3 + b] * vs[1] + bC[6 + b] * vs[2]);
+    for (int b = 0; b < 3; ++b) px[b] -= inv_dx * (cbC[b] * vs[0] + cbC[3 + b] * vs[1] + cbC[6 + b] * vs[2]);
     if (tri) {
       const long long nt = B.nt;
 #pragma unroll
@@ -723,17 +743,14 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
 #pragma unroll
       for (int a = 0; a < 3; ++a) aa[a * n + idx] = bx[a] + px[a];
     }
-#pragma unroll
-    for (int q = 0; q < 9; ++q) cbC[q] = c4 * bC[q];
   }
-  // dL/dv_out at a node: W (dL/dv' + 4 inv_dx dL/dC dpos), dpos in cells
+  // dL/dv_out at a node: W (dL/dv' + 4 inv_dx dL/dC dpos) = W (Kg + cbC o)
   warp_scatter<false>(B, I, ch.inst, st.base, valid, [=](int oi, int oj, int ok) -> float4 {
-    const float W = st.w[0][oi] * st.w[1][oj] * st.w[2][ok];
-    const float px = (float)oi - st.fx[0], py = (float)oj - st.fx[1], pz = (float)ok - st.fx[2];
+    const float W = (st.w[0][oi] * st.w[1][oj]) * st.w[2][ok];
     float4 val;
-    val.x = W * (bV[0] + (cbC[0] * px + cbC[1] * py + cbC[2] * pz));
-    val.y = W * (bV[1] + (cbC[3] * px + cbC[4] * py + cbC[5] * pz));
-    val.z = W * (bV[2] + (cbC[6] * px + cbC[7] * py + cbC[8] * pz));
+    val.x = W * add_off(add_off(add_off(Kg[0], oi, cbC[0]), oj, cbC[1]), ok, cbC[2]);
+    val.y = W * add_off(add_off(add_off(Kg[1], oi, cbC[3]), oj, cbC[4]), ok, cbC[5]);
+    val.z = W * add_off(add_off(add_off(Kg[2], oi, cbC[6]), oj, cbC[7]), ok, cbC[8]);
     val.w = 0.f;
     return val;
   });
@@ -827,39 +844,64 @@ __global__ void __launch_bounds__(256, 3) k_point_adj(BatchDev B, const float* _
   } else {
     m = I.m_c;
   }
-  float Cm[9];
-#pragma unroll
-  for (int q = 0; q < 9; ++q) Cm[q] = __ldg(ai + (6 + q) * n + p);
+  // the APIC payload m (v + C dpos) of a node is K + Cd o with Cd = m dx C and
+  // K = m v - Cd fx; sum W bp dpos comes from the moments mo = sum W bp o
+  // (both as in k_tri_adj)
   const float dx = I.dx, inv_dx = I.inv_dx;
+  float Cd[9], K[3];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) Cd[q] = (m * dx) * __ldg(ai + (6 + q) * n + p);
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+    K[a] = base_v[a] - (Cd[3 * a] * st.fx[0] + Cd[3 * a + 1] * st.fx[1] + Cd[3 * a + 2] * st.fx[2]);
+  float ed[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int o = 0; o < 3; ++o) ed[a][o] = st.dw[a][o] * inv_dx;
   float sp[3] = {0.f, 0.f, 0.f};     // sum W bp
-  float spd[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // sum W bp (x) dpos
+  float mo[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // sum W bp (x) o
   float px[3] = {0.f, 0.f, 0.f};
   const float4* gnb = B.grid_adj + I.node_off;
   const NodeOffsets nofs = node_offsets(I, st.base);
 #pragma unroll
-  for (int q = 0; q < 27; ++q) {
-    const int oi = q / 9, oj = (q / 3) % 3, ok = q % 3;
-    const float w0 = st.w[0][oi], w1 = st.w[1][oj], w2 = st.w[2][ok];
-    const float W = w0 * w1 * w2;
-    const float gW[3] = {st.dw[0][oi] * w1 * w2 * inv_dx, w0 * st.dw[1][oj] * w2 * inv_dx, w0 * w1 * st.dw[2][ok] * inv_dx};
-    const float dp[3] = {((float)oi - st.fx[0]) * dx, ((float)oj - st.fx[1]) * dx, ((float)ok - st.fx[2]) * dx};
-    const float4 g = __ldg(gnb + (nofs.ax[oi] + nofs.ay[oj] + nofs.az[ok]));
-    const float bp[3] = {g.x, g.y, g.z};
-    float s = g.w * m;
+  for (int oi = 0; oi < 3; ++oi)
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const float pay = base_v[a] + m * (Cm[3 * a] * dp[0] + Cm[3 * a + 1] * dp[1] + Cm[3 * a + 2] * dp[2]);
-      s += bp[a] * pay;
-      sp[a] += W * bp[a];
+    for (int oj = 0; oj < 3; ++oj) {
+      const float w0 = st.w[0][oi], w1 = st.w[1][oj];
+      const float w01 = w0 * w1, e0w1 = ed[0][oi] * w1, w0e1 = w0 * ed[1][oj];
+      float kij[3];
 #pragma unroll
-      for (int b = 0; b < 3; ++b) spd[3 * a + b] += W * bp[a] * dp[b];
+      for (int a = 0; a < 3; ++a) kij[a] = add_off(add_off(K[a], oi, Cd[3 * a]), oj, Cd[3 * a + 1]);
+#pragma unroll
+      for (int ok = 0; ok < 3; ++ok) {
+        const float w2 = st.w[2][ok];
+        const float W = w01 * w2;
+        const float gW[3] = {e0w1 * w2, w0e1 * w2, w01 * ed[2][ok]};
+        const float4 g = __ldg(gnb + (nofs.ax[oi] + nofs.ay[oj] + nofs.az[ok]));
+        const float bp[3] = {g.x, g.y, g.z};
+        float s = g.w * m;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          s += bp[a] * add_off(kij[a], ok, Cd[3 * a + 2]);
+          const float Wb = W * bp[a];
+          sp[a] += Wb;
+          mo[3 * a] = add_off(mo[3 * a], oi, Wb);
+          mo[3 * a + 1] = add_off(mo[3 * a + 1], oj, Wb);
+          mo[3 * a + 2] = add_off(mo[3 * a + 2], ok, Wb);
+        }
+#pragma unroll
+        for (int b = 0; b < 3; ++b) px[b] += s * gW[b];
+      }
     }
+  float spd[9];  // sum W bp (x) dpos
 #pragma unroll
-    for (int b = 0; b < 3; ++b) px[b] += s * gW[b];
-  }
-  // - sum_nodes W m C^T bp = - m C^T sp
+  for (int a = 0; a < 3; ++a)
 #pragma unroll
-  for (int b = 0; b < 3; ++b) px[b] -= m * (Cm[b] * sp[0] + Cm[3 + b] * sp[1] + Cm[6 + b] * sp[2]);
+    for (int b = 0; b < 3; ++b) spd[3 * a + b] = dx * (mo[3 * a + b] - st.fx[b] * sp[a]);
+  // - sum_nodes W m C^T bp = - m C^T sp = - Cd^T sp / dx
+#pragma unroll
+  for (int b = 0; b < 3; ++b) px[b] -= inv_dx * (Cd[b] * sp[0] + Cd[3 + b] * sp[1] + Cd[6 + b] * sp[2]);
 #pragma unroll
   for (int a = 0; a < 3; ++a) aa[a * n + p] += px[a];
 #pragma unroll
@@ -971,7 +1013,7 @@ __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* 
         const float d0w1 = ddc[oi] * w1, w0d1 = w0 * ddc[oj];
         float kij[3];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) kij[a] = K[a] + (float)oi * Cm[3 * a] + (float)oj * Cm[3 * a + 1];
+        for (int a = 0; a < 3; ++a) kij[a] = add_off(add_off(K[a], oi, Cm[3 * a]), oj, Cm[3 * a + 1]);
 #pragma unroll
         for (int ok = 0; ok < 3; ++ok) {
           const float w2 = st.w[2][ok], e2 = ed[2][ok];
@@ -985,12 +1027,12 @@ __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* 
           float s = ga.w * m;
 #pragma unroll
           for (int a = 0; a < 3; ++a) {
-            s += bp[a] * (kij[a] + (float)ok * Cm[3 * a + 2]);
+            s += bp[a] * add_off(kij[a], ok, Cm[3 * a + 2]);
             const float Wb = W * bp[a];
             sp[a] += Wb;
-            if (oi) mo[3 * a] += (float)oi * Wb;
-            if (oj) mo[3 * a + 1] += (float)oj * Wb;
-            if (ok) mo[3 * a + 2] += (float)ok * Wb;
+            mo[3 * a] = add_off(mo[3 * a], oi, Wb);
+            mo[3 * a + 1] = add_off(mo[3 * a + 1], oj, Wb);
+            mo[3 * a + 2] = add_off(mo[3 * a + 2], ok, Wb);
             g3[a] += gdot * bp[a];
             sg[a] += sP * gW[a];
           }
