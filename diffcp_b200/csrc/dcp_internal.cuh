@@ -199,28 +199,36 @@ __device__ __forceinline__ void mark_block(long long node, unsigned* flags, int*
 }
 
 // ------------------------------------------------------------ warp scatter
-// Particle-centric scatter of 27-node stencils with warp aggregation.  The
+// Particle-centric scatter of 27-node stencils, one vector atomic
+// (red.global.add.v4.f32, resolved in L2) per issuing lane and node.  The
 // particles of a chunk are in Morton order of their base cells, so particles
-// sharing a base cell sit in consecutive lanes.  Each run of equal base cells
-// is reduced with shuffles (exact float32 sums, as many shuffle rounds as the
-// longest run needs) and only the run's first lane issues the vector atomic
-// (red.global.add.v4.f32, resolved in L2) for each of the 27 nodes.  MARK also
-// registers the (at most 8) grid blocks the run's stencil touches as active.
-// Every lane of the warp must call it; lanes without a particle pass
-// valid = false.
+// sharing a base cell sit in consecutive lanes, and lanes are merged first:
+// mode 2 adds aligned lane pairs with the same base cell (one shuffle per
+// component), mode 0 reduces each run of equal base cells (as many shuffle
+// rounds as the longest run needs), mode 1 merges nothing.  Sums are exact
+// float32 additions in a fixed order within the warp.  MARK (P2G) also
+// registers the (at most 8) grid blocks an issuing lane's stencil touches as
+// active.  Every lane of the warp must call it; lanes without a particle pass
+// valid = false.  nz = false declares every contribution of the lane zero
+// (an adjoint particle whose weights vanish): its atomics are skipped.
 template <bool MARK, class F>
 __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I, int inst, const int base[3],
-                                             bool valid, F&& contrib) {
+                                             bool valid, bool nz, F&& contrib) {
   const unsigned FULL = 0xffffffffu;
   float4* grid = (MARK ? B.grid_pm : B.grid_adj) + I.node_off;
   const int mode = MARK ? B.scatter_mode : B.adj_scatter_mode;
   if (mode == 2) {
     // pairs: lanes 2i and 2i+1 whose particles share a base cell (neighbours
     // in Morton order often do) add their values with one shuffle per
-    // component and issue one atomic per node; other lanes issue their own
+    // component and issue one atomic per node; other lanes issue their own.
+    // A lane whose pair has only zero contributions (nz false on both) issues
+    // none; the adjoint grid has no mass component, so w is not exchanged.
     const int lane = threadIdx.x & 31;
     const int key = valid ? ((base[0] << 22) | (base[1] << 11) | base[2]) : -1 - lane;
     const bool pair = __shfl_xor_sync(FULL, key, 1) == key;
+    const bool mine = valid && nz;
+    const bool theirs = __shfl_xor_sync(FULL, (int)mine, 1) != 0;
+    const bool pnz = mine || (pair && theirs);
     const bool issue = valid && (!pair || (lane & 1) == 0);
     if (MARK && issue) {
 #pragma unroll
@@ -236,6 +244,7 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
             mark_block(node_index(I, i, j, k), B.flags, B.list_blk, B.list_inst, B.counters, inst);
           }
     }
+    if (!__any_sync(FULL, mine)) return;
     const NodeOffsets no = node_offsets(I, base);
 #pragma unroll
     for (int oi = 0; oi < 3; ++oi)
@@ -243,14 +252,15 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
       for (int oj = 0; oj < 3; ++oj)
 #pragma unroll
         for (int ok = 0; ok < 3; ++ok) {
-          float4 v = valid ? contrib(oi, oj, ok) : make_float4(0.f, 0.f, 0.f, 0.f);
+          float4 v = mine ? contrib(oi, oj, ok) : make_float4(0.f, 0.f, 0.f, 0.f);
           const float x = __shfl_xor_sync(FULL, v.x, 1), y = __shfl_xor_sync(FULL, v.y, 1);
-          const float z = __shfl_xor_sync(FULL, v.z, 1), w = __shfl_xor_sync(FULL, v.w, 1);
+          const float z = __shfl_xor_sync(FULL, v.z, 1);
+          const float w = MARK ? __shfl_xor_sync(FULL, v.w, 1) : 0.f;
           if (pair) {
-            v.x += x; v.y += y; v.z += z; v.w += w;
+            v.x += x; v.y += y; v.z += z;
+            if (MARK) v.w += w;
           }
-          if (issue && (v.x != 0.f || v.y != 0.f || v.z != 0.f || v.w != 0.f))
-            atomicAdd(grid + (no.ax[oi] + no.ay[oj] + no.az[ok]), v);
+          if (issue && pnz) atomicAdd(grid + (no.ax[oi] + no.ay[oj] + no.az[ok]), v);
         }
     return;
   }
@@ -270,17 +280,14 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
             mark_block(node_index(I, i, j, k), B.flags, B.list_blk, B.list_inst, B.counters, inst);
           }
     }
+    if (!nz) return;
     const NodeOffsets no = node_offsets(I, base);
 #pragma unroll
     for (int oi = 0; oi < 3; ++oi)
 #pragma unroll
       for (int oj = 0; oj < 3; ++oj)
 #pragma unroll
-        for (int ok = 0; ok < 3; ++ok) {
-          const float4 v = contrib(oi, oj, ok);
-          if (v.x != 0.f || v.y != 0.f || v.z != 0.f || v.w != 0.f)
-            atomicAdd(grid + (no.ax[oi] + no.ay[oj] + no.az[ok]), v);
-        }
+        for (int ok = 0; ok < 3; ++ok) atomicAdd(grid + (no.ax[oi] + no.ay[oj] + no.az[ok]), contrib(oi, oj, ok));
     return;
   }
   const int lane = threadIdx.x & 31;
@@ -336,7 +343,7 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
           }
         }
         if (head && valid && (v.x != 0.f || v.y != 0.f || v.z != 0.f || v.w != 0.f))
-          atomicAdd(grid + (no.ax[oi] + no.ay[oj] + no.az[ok]), v);
+          atomicAdd(grid + (no.ax[oi] + no.ay[oj] + no.az[ok]), v);  // (runs check each node: nz unused)
       }
 }
 

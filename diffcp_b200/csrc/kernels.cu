@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(256, MINB) k_tri_forward(BatchDev B, const flo
     }
   }
   // own-node APIC momentum, mass and normal force (simulation.py:250-265)
-  warp_scatter<true>(B, I, ch.inst, st.base, valid, [=](int oi, int oj, int ok) -> float4 {
+  warp_scatter<true>(B, I, ch.inst, st.base, valid, true, [=](int oi, int oj, int ok) -> float4 {
     const float w0 = st.w[0][oi], w1 = st.w[1][oj], w2 = st.w[2][ok];
     const float w01 = w0 * w1;
     const float W = w01 * w2;
@@ -346,7 +346,7 @@ __global__ void __launch_bounds__(256) k_point_p2g(BatchDev B, const float* __re
       K[a] = base_v[a] - (A[3 * a] * st.fx[0] + A[3 * a + 1] * st.fx[1] + A[3 * a + 2] * st.fx[2]);
     }
   }
-  warp_scatter<true>(B, I, ch.inst, st.base, valid, [=](int oi, int oj, int ok) -> float4 {
+  warp_scatter<true>(B, I, ch.inst, st.base, valid, true, [=](int oi, int oj, int ok) -> float4 {
     const float W = (st.w[0][oi] * st.w[1][oj]) * st.w[2][ok];
     float4 val;
     val.x = W * add_off(add_off(add_off(K[0], oi, A[0]), oj, A[1]), ok, A[2]);
@@ -576,7 +576,8 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
   const long long idx = ch.start + tid;
   Sten st;
   float gdamp[1] = {0.f};
-  float bV[3] = {0.f, 0.f, 0.f}, cbC[9], Kg[3] = {0.f, 0.f, 0.f};  // dL/dv', 4/dx dL/dC, node weight base
+  float bV[3] = {0.f, 0.f, 0.f}, Kg[3] = {0.f, 0.f, 0.f};  // dL/dv', node weight base
+  float cbC[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // 4/dx dL/dC of the gather
   if (valid) {
     float X[3];
     float *ai = nullptr, *ao = nullptr, *aa = nullptr;
@@ -746,8 +747,14 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
       for (int a = 0; a < 3; ++a) aa[a * n + idx] = bx[a] + px[a];
     }
   }
-  // dL/dv_out at a node: W (dL/dv' + 4 inv_dx dL/dC dpos) = W (Kg + cbC o)
-  warp_scatter<false>(B, I, ch.inst, st.base, valid, [=](int oi, int oj, int ok) -> float4 {
+  // dL/dv_out at a node: W (dL/dv' + 4 inv_dx dL/dC dpos) = W (Kg + cbC o),
+  // zero at every node when Kg and cbC are
+  bool nz = false;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) nz = nz || Kg[a] != 0.f;
+#pragma unroll
+  for (int q = 0; q < 9; ++q) nz = nz || cbC[q] != 0.f;
+  warp_scatter<false>(B, I, ch.inst, st.base, valid, nz, [=](int oi, int oj, int ok) -> float4 {
     const float W = (st.w[0][oi] * st.w[1][oj]) * st.w[2][ok];
     float4 val;
     val.x = W * add_off(add_off(add_off(Kg[0], oi, cbC[0]), oj, cbC[1]), ok, cbC[2]);
@@ -1070,6 +1077,9 @@ __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* 
     for (int c = 0; c < 3; ++c)
 #pragma unroll
       for (int a = 0; a < 3; ++a) bf[c][a] = B.barf[a * (long long)B.nv + g.vid[c]];
+    // D0^-1 read again rather than held in registers across the stencil loop
+#pragma unroll
+    for (int q = 0; q < 9; ++q) Di[q] = __ldg(R.Di + q * nt + t);
     const float r1[3] = {Di[0], d.m[1], d.m[2]};
     const float r2[3] = {Di[3], d.m[4], d.m[5]};
     M3<float> bP;
