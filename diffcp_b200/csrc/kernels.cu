@@ -177,12 +177,11 @@ __device__ __forceinline__ void lame(float E, float nu, float& mu, float& la) {
 }
 
 // ============================================================== forward
-template <int MINB>
-__global__ void __launch_bounds__(256, MINB) k_tri_forward(BatchDev B, const float* __restrict__ params,
-                                                     const float* __restrict__ rest, const float* __restrict__ sin,
-                                                     const int2* __restrict__ skip, const float* __restrict__ fdev) {
-  if (skip && skip->x >= 0) return;  // the grid of this substep is restored from the tape
-  const Chunk ch = B.chunks[blockIdx.x];
+// One triangle chunk of k_tri_forward.
+__device__ __forceinline__ void tri_forward_chunk(const BatchDev& B, const float* __restrict__ params,
+                                                  const float* __restrict__ rest, const float* __restrict__ sin,
+                                                  const float* __restrict__ fdev, int c) {
+  const Chunk ch = B.chunks[c];
   const InstDev& I = B.inst[ch.inst];
   const int tid = threadIdx.x;
   const bool valid = tid < ch.count;
@@ -263,6 +262,17 @@ __global__ void __launch_bounds__(256, MINB) k_tri_forward(BatchDev B, const flo
   });
 }
 
+// Triangle P2G.  A full launch has one CTA per chunk; the adjoint substep's
+// launch, which returns at once when the tape holds the substep's grid, has a
+// few CTAs per SM that stride over the chunks otherwise.
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_tri_forward(BatchDev B, const float* __restrict__ params,
+                                                     const float* __restrict__ rest, const float* __restrict__ sin,
+                                                     const int2* __restrict__ skip, const float* __restrict__ fdev) {
+  if (skip && skip->x >= 0) return;  // the grid of this substep is restored from the tape
+  for (int c = blockIdx.x; c < B.n_tri_chunks; c += gridDim.x) tri_forward_chunk(B, params, rest, sin, fdev, c);
+}
+
 __device__ __forceinline__ void point_arrays(const BatchDev& B, const StateP& S, int kind, float*& base, long long& n) {
   if (kind == CHUNK_VERTEX) { base = S.v; n = B.nv; }
   else if (kind == CHUNK_OPERATOR) { base = S.o; n = B.no; }
@@ -289,12 +299,12 @@ __device__ __forceinline__ bool operator_velocity(const BatchDev& B, const InstD
   return false;
 }
 
-__global__ void __launch_bounds__(256) k_point_p2g(BatchDev B, const float* __restrict__ traj, int step, int window,
-                                                   const float* __restrict__ rest, const float* __restrict__ sin,
-                                                   const int2* __restrict__ skip, float* __restrict__ fv_out,
-                                                   int clear_forces) {
-  if (skip && skip->x >= 0) return;  // the grid of this substep is restored from the tape
-  const Chunk ch = B.chunks[B.n_tri_chunks + blockIdx.x];
+// One point chunk (vertex, operator or cube) of k_point_p2g.
+__device__ __forceinline__ void point_p2g_chunk(const BatchDev& B, const float* __restrict__ traj, int step,
+                                                int window, const float* __restrict__ rest,
+                                                const float* __restrict__ sin, float* __restrict__ fv_out,
+                                                int clear_forces, int c) {
+  const Chunk ch = B.chunks[B.n_tri_chunks + c];
   const InstDev& I = B.inst[ch.inst];
   const int tid = threadIdx.x;
   const bool valid = tid < ch.count;
@@ -357,6 +367,16 @@ __global__ void __launch_bounds__(256) k_point_p2g(BatchDev B, const float* __re
   });
   // cleared after all loads of the kernel, ready for the next substep's sums
   if (clear_forces && valid && ch.kind == CHUNK_VERTEX) B.fvert[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// Point P2G; launch shapes as for k_tri_forward.
+__global__ void __launch_bounds__(256) k_point_p2g(BatchDev B, const float* __restrict__ traj, int step, int window,
+                                                   const float* __restrict__ rest, const float* __restrict__ sin,
+                                                   const int2* __restrict__ skip, float* __restrict__ fv_out,
+                                                   int clear_forces) {
+  if (skip && skip->x >= 0) return;  // the grid of this substep is restored from the tape
+  for (int c = blockIdx.x; c < B.n_point_chunks; c += gridDim.x)
+    point_p2g_chunk(B, traj, step, window, rest, sin, fv_out, clear_forces, c);
 }
 
 // Node coordinates of lane l (0..63) of an active block.
@@ -1414,12 +1434,17 @@ cudaError_t launch_backward(const BatchDev& B, const LaunchCfg& L, const float* 
   const int2* meta = T ? T->meta + step : nullptr;
   cudaMemsetAsync(B.counters, 0, sizeof(int), s);
   if (T) DCP_LAUNCH(KID_TAPE, (k_tape_restore<<<L.grid_ctas, 256, 0, s>>>(B, *T, step)));
+  // with a tape the P2G recompute usually returns at once: launch a few CTAs
+  // per SM that stride over the chunks instead of one CTA per chunk
+  const int stride_ctas = 2 * L.grid_ctas;
+  const int tri_ctas = T && B.n_tri_chunks > stride_ctas ? stride_ctas : B.n_tri_chunks;
+  const int point_ctas = T && B.n_point_chunks > stride_ctas ? stride_ctas : B.n_point_chunks;
   if (B.n_tri_chunks)
-    DCP_LAUNCH(KID_TRI_FORWARD, (DCP_MINB(k_tri_forward, L, 0)<<<B.n_tri_chunks, L.block, 0, s>>>(
+    DCP_LAUNCH(KID_TRI_FORWARD, (DCP_MINB(k_tri_forward, L, 0)<<<tri_ctas, L.block, 0, s>>>(
                                     B, params, rest, sin, meta, nullptr)));
   if (B.n_point_chunks)
-    DCP_LAUNCH(KID_POINT_P2G, (k_point_p2g<<<B.n_point_chunks, L.block, 0, s>>>(B, traj, step, window, rest, sin,
-                                                                               meta, nullptr, 0)));
+    DCP_LAUNCH(KID_POINT_P2G, (k_point_p2g<<<point_ctas, L.block, 0, s>>>(B, traj, step, window, rest, sin,
+                                                                         meta, nullptr, 0)));
   DCP_LAUNCH(KID_GRID, (k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_RECOMPUTE, none)));
   DCP_LAUNCH(KID_G2P_ADJ, (DCP_MINB(k_g2p_adj, L, 1)<<<B.n_tri_chunks + B.n_point_chunks, L.block, 0, s>>>(
                               B, params, rest, sin, aout, ain, gparams, snext)));
