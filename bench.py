@@ -204,7 +204,7 @@ def profile_substeps(args):
     Launch order of the second rollout, per substep: forward k_tri_forward,
     k_point_p2g, k_tape_reserve, k_grid, k_g2p x2; adjoint k_tape_restore,
     k_tri_forward and k_point_p2g (both return at once), k_grid, k_g2p_adj,
-    k_grid_adj, k_point_adj, k_tri_adj, k_vertex_collect."""
+    k_grid_adj, k_point_adj, k_tri_adj (and k_vertex_collect after substep 0)."""
     import torch
     from diffcp_b200 import autotune
     from diffcp_b200.batch import BatchSim, ClothBatch

@@ -561,8 +561,11 @@ int dcp_rollout_backward(DcpBatch* b, const float* params, const float* traj, co
         // state f + 1: inside the segment, or the next checkpoint / final state
         const long long nslot = f < last ? -2 : ckpt_slot(f + 1, n, K);
         const float* snext = f < last ? state_at(f + 1) : (nslot >= 0 ? buf + nslot * S : nullptr);
+        // the triangles' per-vertex adjoint sums pass to the next adjoint
+        // substep, which adds them to the vertex adjoints it reads; the last
+        // substep (f = 0) adds them to the returned adjoint
         cudaError_t e = launch_backward(b->B, b->L, params, traj, rest, f, window, state_at(f), adj + so * S,
-                                        adj + (1 - so) * S, gparams, gtraj, s, tp, snext);
+                                        adj + (1 - so) * S, gparams, gtraj, s, tp, snext, f != Lstep - 1, f == 0);
         if (e != cudaSuccess) return e;
       }
     }

@@ -81,10 +81,14 @@ cudaError_t launch_reset(const BatchDev& B, const LaunchCfg& L, float* rest, flo
                          cudaStream_t s);
 // snext (optional): the state after this substep, as the forward produced it;
 // the triangles' damped C is read from it instead of being gathered again.
+// collect = false leaves the triangles' per-vertex adjoint sums of this
+// substep out of ain; the next adjoint substep, given fold = true, adds them
+// to the vertex adjoints it reads (its aout) and clears them.  A chain of
+// substeps folds in every substep after the first and collects in the last.
 cudaError_t launch_backward(const BatchDev& B, const LaunchCfg& L, const float* params, const float* traj,
                             const float* rest, int step, int window, const float* sin, const float* aout, float* ain,
                             double* gparams, double* gtraj, cudaStream_t s, const TapeP* T = nullptr,
-                            const float* snext = nullptr);
+                            const float* snext = nullptr, bool fold = false, bool collect = true);
 cudaError_t launch_chamfer_forward(const BatchDev& B, const LaunchCfg& L, int max_nq, const float* rest,
                                    const float* state, const float* targets, int* qarg, float* loss, cudaStream_t s);
 cudaError_t launch_chamfer_backward(const BatchDev& B, const LaunchCfg& L, int max_nq, const float* rest,

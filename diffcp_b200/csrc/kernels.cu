@@ -582,7 +582,8 @@ template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* __restrict__ params,
                                                  const float* __restrict__ rest, const float* __restrict__ sin,
                                                  const float* __restrict__ aout, float* __restrict__ ain,
-                                                 double* __restrict__ gparams, const float* __restrict__ snext) {
+                                                 double* __restrict__ gparams, const float* __restrict__ snext,
+                                                 int fold) {
   const Chunk ch = B.chunks[blockIdx.x];
   const InstDev& I = B.inst[ch.inst];
   const int tid = threadIdx.x;
@@ -703,10 +704,18 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
         for (int b = 0; b < 3; ++b)
           bC[3 * a + b] = 0.5f * (bCn[3 * a + b] - bCn[3 * b + a]) + keep * 0.5f * (bCn[3 * a + b] + bCn[3 * b + a]);
     } else {
+      float sum_x[3] = {0.f, 0.f, 0.f}, sum_v[3] = {0.f, 0.f, 0.f};
+      if (fold && ch.kind == CHUNK_VERTEX) {
+        // the triangles' per-vertex sums of the previous adjoint substep,
+        // still to be added to this vertex's position / velocity adjoint
+        const float4 sx = B.vadj[idx], sv = B.vadj[B.nv + idx];
+        sum_x[0] = sx.x; sum_x[1] = sx.y; sum_x[2] = sx.z;
+        sum_v[0] = sv.x; sum_v[1] = sv.y; sum_v[2] = sv.z;
+      }
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        bx[a] = __ldg(ao + a * n + idx);
-        bV[a] = __ldg(ao + (3 + a) * n + idx) + dt * bx[a];
+        bx[a] = __ldg(ao + a * n + idx) + sum_x[a];
+        bV[a] = (__ldg(ao + (3 + a) * n + idx) + sum_v[a]) + dt * bx[a];
       }
 #pragma unroll
       for (int q = 0; q < 9; ++q) bC[q] = __ldg(ao + (6 + q) * n + idx);
@@ -784,6 +793,12 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
     return val;
   });
   if (tri) block_sum_atomic<1>(gdamp, gparams + ch.inst * PRM_STRIDE + PRM_DAMPING);
+  // folded sums cleared after all of the kernel's loads (a store before them
+  // makes them wait), ready for this substep's k_tri_adj
+  if (fold && valid && ch.kind == CHUNK_VERTEX) {
+    B.vadj[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
+    B.vadj[B.nv + idx] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
 }
 
 // Reverse of k_grid: dL/dp, dL/dm of every active node from dL/dv_out.
@@ -961,7 +976,8 @@ __global__ void __launch_bounds__(256, 3) k_point_adj(BatchDev B, const float* _
 // Reverse of k_tri_forward for one triangle: own-stencil gather, per-corner
 // force adjoints from dL/df of the three vertices, stress adjoint, and the
 // contributions to the three vertices (summed per vertex, added to the vertex
-// adjoint by k_vertex_collect).
+// adjoint by k_vertex_collect or, inside a rollout, by the next adjoint
+// substep's k_g2p_adj).
 template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* __restrict__ params,
                                                  const float* __restrict__ rest, const float* __restrict__ sin,
@@ -1429,7 +1445,8 @@ cudaError_t launch_forward(const BatchDev& B, const LaunchCfg& L, const float* p
 
 cudaError_t launch_backward(const BatchDev& B, const LaunchCfg& L, const float* params, const float* traj,
                             const float* rest, int step, int window, const float* sin, const float* aout, float* ain,
-                            double* gparams, double* gtraj, cudaStream_t s, const TapeP* T, const float* snext) {
+                            double* gparams, double* gtraj, cudaStream_t s, const TapeP* T, const float* snext,
+                            bool fold, bool collect) {
   const TapeP none = no_tape();
   const int2* meta = T ? T->meta + step : nullptr;
   cudaMemsetAsync(B.counters, 0, sizeof(int), s);
@@ -1447,7 +1464,7 @@ cudaError_t launch_backward(const BatchDev& B, const LaunchCfg& L, const float* 
                                                                          meta, nullptr, 0)));
   DCP_LAUNCH(KID_GRID, (k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_RECOMPUTE, none)));
   DCP_LAUNCH(KID_G2P_ADJ, (DCP_MINB(k_g2p_adj, L, 1)<<<B.n_tri_chunks + B.n_point_chunks, L.block, 0, s>>>(
-                              B, params, rest, sin, aout, ain, gparams, snext)));
+                              B, params, rest, sin, aout, ain, gparams, snext, fold ? 1 : 0)));
   DCP_LAUNCH(KID_GRID_ADJ, (k_grid_adj<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, gparams, gtraj)));
   if (B.n_point_chunks)
     DCP_LAUNCH(KID_POINT_ADJ, (k_point_adj<<<B.n_point_chunks, L.block, 0, s>>>(
@@ -1456,7 +1473,8 @@ cudaError_t launch_backward(const BatchDev& B, const LaunchCfg& L, const float* 
   if (B.n_tri_chunks)
     DCP_LAUNCH(KID_TRI_ADJ, (DCP_MINB(k_tri_adj, L, 2)<<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin, ain,
                                                                                         gparams)));
-  if (B.nv) DCP_LAUNCH(KID_VERTEX_COLLECT, (k_vertex_collect<<<ceil_div(B.nv, 256), 256, 0, s>>>(B, ain)));
+  if (B.nv && collect)
+    DCP_LAUNCH(KID_VERTEX_COLLECT, (k_vertex_collect<<<ceil_div(B.nv, 256), 256, 0, s>>>(B, ain)));
   return cudaGetLastError();
 }
 
