@@ -1,6 +1,8 @@
 // sm_100a kernels of the batched codimensional-cloth MPM substep, its adjoint
-// and the Chamfer loss.  One CTA processes one chunk: a contiguous,
-// mesh-ordered range of one particle species of one cloth instance.
+// and the Chamfer loss.  One CTA processes one chunk: a contiguous range of
+// one particle species of one cloth instance, in Morton order of the
+// particles' stencil base cells (the adjoint substep's P2G launches stride a
+// smaller grid over the chunks).
 //
 // Forward substep (simulation.py:480-488, forward):
 //   k_tri_forward    in-plane QR + rotation factor + stress of every triangle
@@ -17,7 +19,9 @@
 //                    blocks only
 //   k_g2p            G2P for all species + triangle state update
 //                    (simulation.py:304-430)
-// Reverse substep: k_g2p_adj, k_grid_adj, k_point_adj, k_tri_adj, k_vertex_collect.
+// Reverse substep: k_g2p_adj, k_grid_adj, k_point_adj, k_tri_adj; k_vertex_collect
+// after a single substep or after a rollout's last one (inside a rollout the
+// next substep's k_g2p_adj takes in the triangles' per-vertex adjoint sums).
 // Grid tape (optional): k_tape_reserve / k_tape_restore keep each forward
 // substep's particle-to-grid result so that the reverse substep skips P2G.
 // Replay (forward only, simulation_without_grad.py): k_reset_tri /
