@@ -10,12 +10,19 @@
 // in a file-scope device array of fixed size that every GPU loading this
 // library holds until the process exits.
 //
-// The caller still provides every input and output buffer.  The array's
-// device address is fetched once per device with cudaGetSymbolAddress on the
-// first call made with that device current; that first call should therefore
-// come before any stream capture.  All calls share the one array: two calls
-// that overlap on the GPU (for example on two streams) race on it.  Nothing in
-// it needs to start at zero: each call writes the entries it later reads.
+// The caller still provides every input and output buffer.  A __device__
+// array has one address per CUDA context, so the address is looked up with
+// cudaGetSymbolAddress the first time a call runs in a context (the primary
+// context of a device, or a context the host application created with the
+// driver API and made current) and cached under that context's unique id
+// (cuCtxGetId), which the driver never hands out twice in a process.  A
+// context destroyed and created again (cudaDeviceReset, for example) gets a
+// new id, so its first call looks the address up afresh.  The first call in a
+// context should therefore come before any stream capture in it.  All calls in
+// a context share the one array: two calls that overlap on the GPU (for
+// example on two streams) race on it.  Nothing in it needs to start at zero:
+// each call writes the entries it later reads.
+#include <cuda.h>  // driver API types only; the two functions used are fetched with cudaGetDriverEntryPoint
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -31,13 +38,30 @@ static __device__ __align__(256) float g_chamfer_scratch[DCP_STATIC_MAX_TARGETS]
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-float* g_scratch_addr[kMaxDevices] = {nullptr};
+// Scratch address per CUDA context, keyed by the context's unique id.  Ids
+// are never reused, so an entry of a destroyed context is never matched again;
+// the table keeps the most recent kMaxContexts entries.
+constexpr int kMaxContexts = 64;
+struct ScratchEntry {
+  unsigned long long ctx_id;
+  float* addr;
+};
+ScratchEntry g_scratch[kMaxContexts];
+int g_scratch_n = 0, g_scratch_next = 0;
 std::mutex g_scratch_mu;
 
-// Per target: min over vertices of |x - t|^2 / 3 with x = x0 + u, the
-// reference's float32 operation order (parameter_fitting_functions.py:7-14),
-// first vertex index on ties.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+
+// Per target: min over vertices of |x - t|^2 / 3 (parameter_fitting_functions.py:7-14),
+// first vertex index on ties.  The difference x - t is formed rest-relative,
+// (x0 - t) + u, with explicitly rounded float32 operations; the reference
+// subtracts the target from a stored absolute position, so the two round
+// differently.  NaN distances are skipped; a target with no distance below
+// +inf (every vertex non-finite) gets a NaN minimum and argmin -1, so the
+// loss becomes NaN.
 __global__ void __launch_bounds__(128) k_static_min(const float* __restrict__ x0, const float* __restrict__ u, int nv,
                                                     const float* __restrict__ targets, int nq,
                                                     float* __restrict__ qmin, int* __restrict__ argmin) {
@@ -81,7 +105,7 @@ __global__ void __launch_bounds__(128) k_static_min(const float* __restrict__ x0
     __syncthreads();
   }
   if (valid) {
-    qmin[q] = best;
+    qmin[q] = bv >= 0 ? best : __int_as_float(0x7fc00000);
     argmin[q] = bv;
   }
 }
@@ -102,29 +126,67 @@ __global__ void k_static_sum(const float* __restrict__ qmin, int nq, float* __re
   }
 }
 
-int scratch_for_current_device(float** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) {
-    dcp::set_last_error(std::string("dcp_chamfer_forward_static: cudaGetDevice: ") + cudaGetErrorString(e));
+int fail_cuda(const char* what, cudaError_t e) {
+  dcp::set_last_error(std::string("dcp_chamfer_forward_static: ") + what + ": " + cudaGetErrorString(e));
+  return DCP_ERR_CUDA;
+}
+
+// Unique id of the calling thread's current context; 0 when none is current.
+int current_context_id(unsigned long long* id) {
+  CUcontext ctx = nullptr;
+  if (g_ctx_get_current(&ctx) != CUDA_SUCCESS) {
+    dcp::set_last_error("dcp_chamfer_forward_static: cuCtxGetCurrent failed");
     return DCP_ERR_CUDA;
   }
-  if (dev < 0 || dev >= kMaxDevices) {
-    dcp::set_last_error("dcp_chamfer_forward_static: device index beyond the supported range");
-    return DCP_ERR_INVALID;
+  *id = 0;
+  if (ctx && g_ctx_get_id(ctx, id) != CUDA_SUCCESS) {
+    dcp::set_last_error("dcp_chamfer_forward_static: cuCtxGetId failed");
+    return DCP_ERR_CUDA;
   }
+  return DCP_OK;
+}
+
+int scratch_for_current_context(float** out) {
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_chamfer_scratch);
-    if (e != cudaSuccess || !p) {
-      dcp::set_last_error(std::string("dcp_chamfer_forward_static: cudaGetSymbolAddress: ") +
-                          cudaGetErrorString(e));
+  if (!g_ctx_get_current || !g_ctx_get_id) {
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = cudaDriverEntryPointSymbolNotFound;
+    cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1);
+    if (e == cudaSuccess) e = cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2);
+    if (e != cudaSuccess) return fail_cuda("cudaGetDriverEntryPoint", e);
+    if (q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2) {
+      dcp::set_last_error("dcp_chamfer_forward_static: the driver lacks cuCtxGetCurrent / cuCtxGetId");
       return DCP_ERR_CUDA;
     }
-    g_scratch_addr[dev] = static_cast<float*>(p);
+    g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+    g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f2);
   }
-  *out = g_scratch_addr[dev];
+  unsigned long long id = 0;
+  int rc = current_context_id(&id);
+  if (rc != DCP_OK) return rc;
+  if (id) {
+    for (int k = 0; k < g_scratch_n; ++k)
+      if (g_scratch[k].ctx_id == id) {
+        *out = g_scratch[k].addr;
+        return DCP_OK;
+      }
+  }
+  // first call in this context (or no context yet: the runtime then makes the
+  // current device's primary context current while it looks the symbol up)
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_chamfer_scratch);
+  if (e != cudaSuccess || !p) return fail_cuda("cudaGetSymbolAddress", e);
+  if (!id) {
+    rc = current_context_id(&id);
+    if (rc != DCP_OK) return rc;
+  }
+  if (id) {
+    g_scratch[g_scratch_next] = ScratchEntry{id, static_cast<float*>(p)};
+    g_scratch_next = (g_scratch_next + 1) % kMaxContexts;
+    if (g_scratch_n < kMaxContexts) ++g_scratch_n;
+  }
+  *out = static_cast<float*>(p);
   return DCP_OK;
 }
 
@@ -146,7 +208,7 @@ extern "C" int dcp_chamfer_forward_static(const float* x0, const float* u, int32
     return DCP_ERR_INVALID;
   }
   float* scratch = nullptr;
-  const int rc = scratch_for_current_device(&scratch);
+  const int rc = scratch_for_current_context(&scratch);
   if (rc != DCP_OK) return rc;
   cudaStream_t s = (cudaStream_t)stream;
   k_static_min<<<(n_target + 127) / 128, 128, 0, s>>>(x0, u, n_vertex, targets, n_target, scratch, argmin);

@@ -1202,8 +1202,12 @@ __global__ void k_vertex_collect(BatchDev B, float* __restrict__ ain) {
 
 // ============================================================== Chamfer
 // compute_loss (parameter_fitting_functions.py:3-15): for every target point
-// the minimum over vertices of |x - t|^2 / 3, evaluated with the reference's
-// float32 operation order; ties go to the vertex of lowest rank.
+// the minimum over vertices of |x - t|^2 / 3; ties go to the vertex of lowest
+// rank.  x - t is formed rest-relative, (x0 - t) + u, with explicitly rounded
+// float32 operations (the reference subtracts the target from a stored
+// absolute position, which rounds differently).  NaN distances are skipped
+// and flag the instance non-finite; a target with no distance below +inf gets
+// a NaN minimum (the instance's loss becomes NaN) and argmin -1.
 __global__ void __launch_bounds__(128) k_chamfer_fwd(BatchDev B, const float* __restrict__ rest,
                                                      const float* __restrict__ state, const float* __restrict__ targets,
                                                      int* __restrict__ qarg) {
@@ -1225,6 +1229,7 @@ __global__ void __launch_bounds__(128) k_chamfer_fwd(BatchDev B, const float* __
   }
   float best = __int_as_float(0x7f800000);
   int brank = 0x7fffffff, bv = -1;
+  bool nan_seen = false;
   for (int base = 0; base < I.nv; base += 256) {
     for (int j = threadIdx.x; j < 256; j += blockDim.x) {
       const int v = base + j;
@@ -1248,6 +1253,7 @@ __global__ void __launch_bounds__(128) k_chamfer_fwd(BatchDev B, const float* __
         const float dy = __fadd_rn(__fsub_rn(sy[j], ty), uy[j]);
         const float dz = __fadd_rn(__fsub_rn(sz[j], tz), uz[j]);
         const float dd = __fdiv_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)), 3.f);
+        nan_seen |= dd != dd;
         if (dd < best || (dd == best && sr[j] < brank)) {
           best = dd;
           brank = sr[j];
@@ -1258,8 +1264,9 @@ __global__ void __launch_bounds__(128) k_chamfer_fwd(BatchDev B, const float* __
     __syncthreads();
   }
   if (valid) {
-    B.qmin[gq] = bv >= 0 ? best : 0.f;
+    B.qmin[gq] = bv >= 0 ? best : __int_as_float(0x7fc00000);
     qarg[gq] = bv >= 0 ? I.v_off + bv : -1;
+    if (nan_seen || bv < 0) atomicOr(B.status + inst, STATUS_NONFINITE);
   }
 }
 

@@ -17,6 +17,8 @@ c_void_p = ctypes.c_void_p
 _fp = ctypes.POINTER(ctypes.c_float)
 
 DCP_OK = 0
+DCP_ERR_INVALID = 1
+DCP_ERR_CUDA = 2
 GRIP_NONE, GRIP_OPERATOR, GRIP_KINEMATIC = 0, 1, 2
 SVD_GRAD = {"exact": 0, "reference": 1}
 STATUS_OUT_OF_DOMAIN, STATUS_NONFINITE = 1, 2

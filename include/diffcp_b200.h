@@ -60,7 +60,7 @@ extern "C" {
 #define DCP_SVD_GRAD_REFERENCE 1 /* clamped SVD backward of simulation.py:44-50,71-94 */
 
 #define DCP_STATUS_OUT_OF_DOMAIN 1 /* a stencil left the grid; clamped */
-#define DCP_STATUS_NONFINITE 2     /* a particle velocity became NaN/Inf */
+#define DCP_STATUS_NONFINITE 2     /* a particle velocity became NaN/Inf, or a Chamfer distance was NaN */
 
 /* One cloth scene; the scalars are the constants of src/initialization.py:79,115-130. */
 typedef struct DcpInstance {
@@ -162,7 +162,9 @@ int dcp_substep_backward(DcpBatch* batch, const float* params, const float* traj
 
 /* compute_loss (parameter_fitting_functions.py:3-15) per instance: one-sided
  * Chamfer sum_q min_p |x_p - t_q|^2 / 3 / Nq on the vertices of `state`.
- * targets: [3][Nq_total]; argmin: [Nq_total] (global vertex index); loss: [n_inst]. */
+ * targets: [3][Nq_total]; argmin: [Nq_total] (global vertex index); loss: [n_inst].
+ * NaN distances are skipped and set DCP_STATUS_NONFINITE; a target whose
+ * distances are all non-finite gets argmin -1 and makes its instance's loss NaN. */
 int dcp_chamfer_forward(DcpBatch* batch, const float* rest, const float* state, const float* targets,
                         int32_t* argmin, float* loss, void* stream);
 /* compute_loss.grad: adds dL/dx of the vertices into adj_state. */
@@ -228,12 +230,17 @@ const char* dcp_last_error(void);
  * allocator owns the GPU's memory, or a latency-bound loop in which an
  * allocation is not allowed.  The scratch (per-target minima) is a file-scope
  * device array of DCP_STATIC_MAX_TARGETS floats that every GPU loading the
- * library holds until exit.  The first call on a device, with that device
- * current, looks up the array's device address (cudaGetSymbolAddress); make
- * that first call before any stream capture.  All calls share the array:
- * calls that overlap on the GPU race.  x0, u (u may be NULL): [3][n_vertex]
- * rest positions and displacements; targets: [3][n_target]; argmin:
- * [n_target] vertex index (first index on ties); loss: one float.  Returns
+ * library holds until exit.  The array has one address per CUDA context: the
+ * first call in a context (the device's primary context, or a context the
+ * caller created with the driver API and made current) looks it up with
+ * cudaGetSymbolAddress and caches it under the context's unique id, so make
+ * that first call before any stream capture; a context created anew (after
+ * cudaDeviceReset, say) is looked up again on its first call.  All calls in a
+ * context share the array: calls that overlap on the GPU race.  x0, u (u may
+ * be NULL): [3][n_vertex] rest positions and displacements; targets:
+ * [3][n_target]; argmin: [n_target] vertex index (first index on ties); loss:
+ * one float.  Non-finite distances are skipped; a target whose distances are
+ * all non-finite gets argmin -1 and makes the loss NaN.  Returns
  * DCP_ERR_INVALID for n_target > DCP_STATIC_MAX_TARGETS. */
 #define DCP_STATIC_MAX_TARGETS (1 << 20)
 int dcp_chamfer_forward_static(const float* x0, const float* u, int32_t n_vertex, const float* targets,
