@@ -25,8 +25,28 @@ Outputs
   ref_replay_f32.npz    the forward-only replay of simulation_without_grad.py
                         (substep blocks with reset_quadrature_particles) and
                         the pose files animation() writes, float32
+  ref_fd_press_f64.npz  central finite differences of the window-0 loss on the
+                        "press" variant of the synthetic scene (the grasp
+                        pushes the sheet's corners down for 300 substeps, so
+                        that the contact term A22 of simulation.py:216-225
+                        engages), reference kernels in float64
+  ref_real_f32.npz      the reference's own scene (data/cloth_mesh.ply,
+                        grasp_traj_array.npy, target_pcd_sample.npy,
+                        rigid_cube_top_face_center_position.npy) with a short
+                        horizon: compute_grad() itself run over 3 grasp
+                        windows of 30 substeps (end-state carry-over of
+                        parameter_fitting_functions.py:40-49), per-window
+                        losses and vertex histories, float32; and the inputs
+                        (PLY bytes, the 4 trajectory frames, the 3 target
+                        windows, the arguments) so that tests rebuild the tree
+  ref_real_fd_f64.npz   the same scene in float64: window 0, the carry-over,
+                        and central finite differences of the window-1 loss
+                        with respect to E, nu, contact/shearing stiffness and
+                        two grasp-trajectory coordinates, the carried-in state
+                        held fixed (the Tape of compute_grad covers one window)
 
-Run:  python tests/golden/make_golden.py  [--ref PATH]   (needs the reference tree)
+Run:  python tests/golden/make_golden.py --ref PATH   (PATH: the reference's
+source tree; or set DIFFCP_REFERENCE)
 """
 from __future__ import annotations
 
@@ -72,6 +92,20 @@ ARGS = {
 }
 PARAMS = {"E": 400.0, "nu": 0.3, "contact_stiffness": 300.0, "shearing_stiffness": 150.0}
 
+# "press" variant: 300 substeps (0.0601 / 2e-4 -> max_steps 301) and a grasp
+# that pushes the corners down, so the sheet is compressed along its normal
+# (R22 < 1) and the contact stiffness matters to the loss.
+ARGS_PRESS = dict(ARGS, grad_update_interval=0.0601)
+PARAMS_PRESS = {"E": 400.0, "nu": 0.3, "contact_stiffness": 1000.0, "shearing_stiffness": 150.0}
+
+# The reference's own scene with a short horizon: 30 substeps per grasp window
+# (0.00301 / 1e-4 -> max_steps 31), frames 0..3 of the grasp trajectory
+# (end_frame 3) and the first REAL_WINDOWS target windows; the other keys are
+# those of the reference's simulation_arguments.json.
+REAL_OVERRIDES = {"grad_update_interval": 0.00301, "end_frame": 3}
+REAL_WINDOWS = 3
+REAL_FRAMES = 4
+
 
 def write_ply(path, v, t):
     v = np.asarray(v, dtype="<f8")
@@ -88,9 +122,11 @@ def write_ply(path, v, t):
         fh.write(rec.tobytes())
 
 
-def scene_arrays():
+def scene_arrays(variant="base"):
     """Jittered 7x7 sheet (raw units), a 2-point grasp trajectory moving the two
-    far corners, 2 windows x 12 target points, a cube marker."""
+    far corners, 2 windows x 12 target points, a cube marker.  variant "press":
+    the same sheet, targets and marker, with a 100-frame trajectory that moves
+    the corners down and inwards."""
     rng = np.random.default_rng(SEED_SCENE)
     n = 7
     ii, kk = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
@@ -113,10 +149,17 @@ def scene_arrays():
     traj += 0.001 * rng.standard_normal(traj.shape)
     target = verts[None, rng.choice(n * n, 12, replace=False)] + 0.02 * rng.standard_normal((2, 12, 3))
     mark = np.array([0.85, 0.09, 0.55])
+    if variant == "press":
+        t = np.arange(100)[:, None]
+        traj = np.stack([c0 + t * np.array([-0.003, -0.0015, -0.002]),
+                         c1 + t * np.array([-0.003, -0.0015, 0.003])], 1)
     return verts, tris, traj, target, mark
 
 
-def build_tree(ref):
+def build_tree(ref, variant="base"):
+    """A temporary copy of the reference's source files with a scene of its
+    own: the synthetic sheet ("base", "press") or the reference's own data
+    with a short horizon ("real")."""
     tmp = tempfile.mkdtemp(prefix="diffcp_ref_")
     os.makedirs(os.path.join(tmp, "src"))
     os.makedirs(os.path.join(tmp, "data"))
@@ -125,9 +168,24 @@ def build_tree(ref):
         if name.endswith(".py"):
             shutil.copy(os.path.join(ref, "src", name), os.path.join(tmp, "src", name))
     open(os.path.join(tmp, "src", "__init__.py"), "w").close()
+    if variant == "real":
+        with open(os.path.join(ref, "src", "simulation_arguments.json")) as fh:
+            args = json.load(fh)
+        args.update(REAL_OVERRIDES)
+        with open(os.path.join(tmp, "src", "simulation_arguments.json"), "w") as fh:
+            json.dump(args, fh)
+        data = os.path.join(ref, "data")
+        shutil.copy(os.path.join(data, "cloth_mesh.ply"), os.path.join(tmp, "data", "cloth_mesh.ply"))
+        shutil.copy(os.path.join(data, "rigid_cube_top_face_center_position.npy"),
+                    os.path.join(tmp, "data", "rigid_cube_top_face_center_position.npy"))
+        np.save(os.path.join(tmp, "data", "grasp_traj_array.npy"),
+                np.load(os.path.join(data, "grasp_traj_array.npy"))[:REAL_FRAMES])
+        np.save(os.path.join(tmp, "data", "target_pcd_sample.npy"),
+                np.load(os.path.join(data, "target_pcd_sample.npy"))[:REAL_WINDOWS])
+        return tmp
     with open(os.path.join(tmp, "src", "simulation_arguments.json"), "w") as fh:
-        json.dump(ARGS, fh)
-    verts, tris, traj, target, mark = scene_arrays()
+        json.dump(ARGS_PRESS if variant == "press" else ARGS, fh)
+    verts, tris, traj, target, mark = scene_arrays(variant)
     write_ply(os.path.join(tmp, "data", "cloth_mesh.ply"), verts, tris)
     np.save(os.path.join(tmp, "data", "grasp_traj_array.npy"), traj)
     np.save(os.path.join(tmp, "data", "target_pcd_sample.npy"), target)
@@ -135,13 +193,15 @@ def build_tree(ref):
     return tmp
 
 
-def import_reference(tree, f64=False):
+def import_reference(tree, f64=False, forward_tape=False):
     sys.path.insert(0, HERE)
     import ti_standin
     import o3d_standin
     import types
     if f64:
         ti_standin.force_f64()
+    if forward_tape:
+        ti_standin.allow_forward_tape()
     sys.modules["taichi"] = ti_standin
     sys.modules["taichi_glsl"] = types.ModuleType("taichi_glsl")
     sys.modules["open3d"] = o3d_standin
@@ -250,6 +310,147 @@ def run_fd64(tree, out):
     np.savez_compressed(out, **rec)
 
 
+def _fd_params(m, base, loss_fn, rel_h=1e-5):
+    """Central differences of loss_fn() in each of the four parameters."""
+    rec = {}
+    for name in ("E", "nu", "contact_stiffness", "shearing_stiffness"):
+        h = rel_h * base[name]
+        vals = []
+        for sgn in (1, -1):
+            p = dict(base)
+            p[name] = base[name] + sgn * h
+            set_params(m, p)
+            vals.append(loss_fn())
+        rec["fd_" + name] = (vals[0] - vals[1]) / (2 * h)
+        set_params(m, base)
+    return rec
+
+
+def run_press64(tree, out):
+    m = import_reference(tree, f64=True)
+    base = dict(PARAMS_PRESS)
+    set_params(m, base)
+    rec = {"loss": window_loss(m, 0)}
+    rec.update(_fd_params(m, base, lambda: window_loss(m, 0), rel_h=1e-4))
+    for (a, b, c) in ((20, 0, 1), (40, 1, 2)):
+        h = 1e-6
+        vals = []
+        for sgn in (1, -1):
+            m.grasp_point_pos[a, b, c] += sgn * h
+            vals.append(window_loss(m, 0))
+            m.grasp_point_pos[a, b, c] -= sgn * h
+        rec["fd_seq_%d_%d_%d" % (a, b, c)] = (vals[0] - vals[1]) / (2 * h)
+    rec["params"] = np.array([base["E"], base["nu"], base["contact_stiffness"], base["shearing_stiffness"]])
+    rec["max_steps"] = np.array(m.max_steps)
+    np.savez_compressed(out, **rec)
+
+
+def _real_initial_params(m):
+    """initial_constitutive_parameters of the arguments (what
+    parameter_fitting_main.py:3-6 sets before fitting)."""
+    return {"E": float(m.initial_garment_E), "nu": float(m.initial_garment_nu),
+            "contact_stiffness": float(m.initial_contact_stiffness),
+            "shearing_stiffness": float(m.initial_shearing_stiffness)}
+
+
+def run_real32(tree, out):
+    """compute_grad() of the reference over the short-horizon real scene; the
+    window histories are read where compute_grad re-initialises the fields
+    from the window's end state (parameter_fitting_functions.py:40-49)."""
+    import contextlib
+    import io
+    m = import_reference(tree, forward_tape=True)
+    base = _real_initial_params(m)
+    set_params(m, base)
+    m.initialize_objects()
+    hist = []
+    orig = m.initialize_ti_field
+
+    def observed():
+        hist.append({k: getattr(m, k).to_numpy() for k in ("vertex_x", "operator_x", "cube_x")})
+        hist[-1]["loss"] = float(m.loss[None])
+        orig()
+
+    m.initialize_ti_field = observed
+    with contextlib.redirect_stdout(io.StringIO()):
+        loss_mean, _ = m.compute_grad()
+    m.initialize_ti_field = orig
+    rec = {"loss_mean": np.array(loss_mean), "n_windows": np.array(len(hist)), "params": np.array(
+        [base["E"], base["nu"], base["contact_stiffness"], base["shearing_stiffness"]])}
+    for g, h in enumerate(hist):
+        rec["w%d_loss" % g] = np.array(h["loss"])
+        rec["w%d_vertex_x" % g] = h["vertex_x"]
+        rec["w%d_operator_x_end" % g] = h["operator_x"][-1]
+        rec["w%d_cube_x_end" % g] = h["cube_x"][-1]
+    for name in ("dt", "n_grid", "vertex_p_mass", "quadrature_p_mass", "quadrature_p_vol", "operator_p_mass",
+                 "cube_p_mass", "garment_surface_area", "max_steps", "n_actions", "grasper_group_size",
+                 "n_grad_updates"):
+        if hasattr(m, name):
+            rec["const_" + name] = np.asarray(getattr(m, name))
+    rec["soft_body_model_vertices"] = np.asarray(m.soft_body_model_vertices)
+    rec["grasp_point_pos"] = np.asarray(m.grasp_point_pos)
+    rec["target_pcd_array"] = np.asarray(m.target_pcd_array)
+    rec["cube_model"] = np.asarray(m.cube_model)
+    rec["operator_model_without_position"] = np.asarray(m.operator_model_without_position)
+    # the inputs, so that tests rebuild the tree without the reference
+    with open(os.path.join(tree, "data", "cloth_mesh.ply"), "rb") as fh:
+        rec["in_ply_bytes"] = np.frombuffer(fh.read(), dtype=np.uint8)
+    for name in ("grasp_traj_array", "target_pcd_sample", "rigid_cube_top_face_center_position"):
+        rec["in_" + name] = np.load(os.path.join(tree, "data", name + ".npy"))
+    with open(os.path.join(tree, "src", "simulation_arguments.json")) as fh:
+        rec["in_arguments_json"] = np.array(fh.read())
+    np.savez_compressed(out, **rec)
+
+
+def run_real64(tree, out):
+    """Window 0, the carry-over of compute_grad (parameter_fitting_functions.py:
+    40-49), and central differences of the window-1 loss with the carried-in
+    state held fixed, in float64."""
+    m = import_reference(tree, f64=True)
+    base = _real_initial_params(m)
+    set_params(m, base)
+    m.initialize_objects()
+    rec = {"w0_loss": window_loss_carry(m, 0)}
+    last = m.max_steps - 1
+    carried = {"op": m.operator_x.to_numpy()[last], "vx": m.vertex_x.to_numpy()[last],
+               "cube": m.cube_x.to_numpy()[last]}
+    faces = np.asarray(m.soft_body_mesh.triangles)
+    rec["w0_vertex_x_end"] = carried["vx"]
+
+    def window1():
+        m.initial_operator_x.from_numpy(carried["op"])
+        m.initial_vertex_x.from_numpy(carried["vx"])
+        m.lagrangian_mesh_element.from_numpy(faces)
+        m.initial_cube_x.from_numpy(carried["cube"])
+        m.initialize_ti_field()
+        return window_loss_carry(m, 1)
+
+    rec["w1_loss"] = window1()
+    rec.update({"w1_" + k: v for k, v in _fd_params(m, base, window1, rel_h=1e-4).items()})
+    for (a, b, c) in ((0, 0, 1), (1, 1, 0)):
+        h = 1e-7
+        vals = []
+        for sgn in (1, -1):
+            m.grasp_tracking_seq[a][b, c] += sgn * h     # the keyframes of this window (set by initialize_objects)
+            vals.append(window1())
+            m.grasp_tracking_seq[a][b, c] -= sgn * h
+        rec["w1_fd_seq_%d_%d_%d" % (a, b, c)] = (vals[0] - vals[1]) / (2 * h)
+    rec["params"] = np.array([base["E"], base["nu"], base["contact_stiffness"], base["shearing_stiffness"]])
+    np.savez_compressed(out, **rec)
+
+
+def window_loss_carry(m, g):
+    """The body of compute_grad for window g from the current fields (no
+    re-initialisation): set targets, substeps 0..max_steps-2, compute_loss."""
+    m.clear_distances()
+    m.target_pos.from_numpy(m.target_pcd_array[g])
+    m.loss[None] = 0
+    for f in range(m.max_steps - 1):
+        m.forward(f, g)
+    m.compute_loss(f)
+    return float(m.loss[None])
+
+
 def run_fitting(tree, out):
     """``single_parameter_fitting`` (parameter_fitting_functions.py:65-92) on
     random and edge inputs, and ``parameters_learning`` (94-205) driven by the
@@ -332,28 +533,41 @@ def run_replay(tree, out):
     np.savez_compressed(out, **rec)
 
 
+MODES = ("forward32", "svd", "fd64", "fitting", "replay", "press64", "real32", "real64")
+VARIANT = {"press64": "press", "real32": "real", "real64": "real"}
+OUT = {"forward32": "ref_forward_f32.npz", "svd": "ref_svd_backward.npz", "fd64": "ref_fd_f64.npz",
+       "fitting": "ref_fitting.npz", "replay": "ref_replay_f32.npz", "press64": "ref_fd_press_f64.npz",
+       "real32": "ref_real_f32.npz", "real64": "ref_real_fd_f64.npz"}
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--mode", default="all", choices=["all", "forward32", "svd", "fd64", "fitting", "replay"])
+    ap.add_argument("--ref", default=os.environ.get("DIFFCP_REFERENCE"),
+                    help="the reference's source tree (default: $DIFFCP_REFERENCE)")
+    ap.add_argument("--mode", default="all", choices=("all",) + MODES)
     ap.add_argument("--tree")
     ap.add_argument("--only", nargs="*", help="with --mode all: the modes to regenerate")
     a = ap.parse_args()
     if a.mode == "all":
-        tree = build_tree(a.ref)
+        if not a.ref:
+            ap.error("--ref (or DIFFCP_REFERENCE) is required")
+        trees = {}
         try:
-            for mode in a.only or ("forward32", "svd", "fd64", "fitting", "replay"):
+            for mode in a.only or MODES:
+                variant = VARIANT.get(mode, "base")
+                if variant not in trees:
+                    trees[variant] = build_tree(a.ref, variant)
                 t0 = time.time()
-                subprocess.run([sys.executable, __file__, "--mode", mode, "--tree", tree], check=True)
+                subprocess.run([sys.executable, __file__, "--mode", mode, "--tree", trees[variant],
+                                "--ref", a.ref], check=True)
                 print("%s done in %.1f s" % (mode, time.time() - t0))
         finally:
-            shutil.rmtree(tree, ignore_errors=True)
+            for tree in trees.values():
+                shutil.rmtree(tree, ignore_errors=True)
         return
-    out = {"forward32": "ref_forward_f32.npz", "svd": "ref_svd_backward.npz", "fd64": "ref_fd_f64.npz",
-           "fitting": "ref_fitting.npz", "replay": "ref_replay_f32.npz"}[a.mode]
+    out = os.path.join(HERE, OUT[a.mode])
     {"forward32": run_forward32, "svd": run_svd, "fd64": run_fd64, "fitting": run_fitting,
-     "replay": run_replay}[a.mode](
-        a.tree, os.path.join(HERE, out))
+     "replay": run_replay, "press64": run_press64, "real32": run_real32, "real64": run_real64}[a.mode](a.tree, out)
 
 
 if __name__ == "__main__":

@@ -190,6 +190,11 @@ class Field:
 
     def __getitem__(self, idx):
         view = self.arr[self._key(idx)]
+        if idx is None and not view.ndim:
+            # a 0-D field read as field[None] is a value, as Taichi returns a
+            # Python number: a view would change when the field is written later
+            return view[()]
+        # element access stays a view: ti.atomic_add(field[i], v) adds through it
         return view.view(TiArr) if view.ndim else view
 
     def __setitem__(self, idx, value):
@@ -299,9 +304,27 @@ def svd(A):
     return U.view(TiArr), np.array([[s1, 0], [0, s2]], dtype=dt).view(TiArr), V.view(TiArr)
 
 
+_FORWARD_TAPE = [False]
+
+
+def allow_forward_tape():
+    """Let ``ti.ad.Tape`` run its body as a plain forward pass (gradient fields
+    stay zero).  The golden generator uses this to drive the reference's
+    ``compute_grad`` for its losses and states; gradients come from finite
+    differences instead."""
+    _FORWARD_TAPE[0] = True
+
+
 class _Tape:
     def __init__(self, loss=None):
-        raise NotImplementedError("Taichi's reverse-mode AD is not emulated by this stand-in")
+        if not _FORWARD_TAPE[0]:
+            raise NotImplementedError("Taichi's reverse-mode AD is not emulated by this stand-in")
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
 
 
 ad = types.SimpleNamespace(

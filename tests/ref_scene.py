@@ -16,9 +16,9 @@ import make_golden as mg  # noqa: E402
 from oracle.scene_ref import reference_scene  # noqa: E402
 
 
-def small_reference_scene():
-    verts, tris, traj, target, mark = mg.scene_arrays()
-    args = mg.ARGS
+def small_reference_scene(variant="base"):
+    verts, tris, traj, target, mark = mg.scene_arrays(variant)
+    args = mg.ARGS_PRESS if variant == "press" else mg.ARGS
     random.seed(mg.SEED_OP)
     np.random.seed(mg.SEED_CUBE)
     n_c = args["rigid_cube_parameters"]["n_rigid_cube_particles"]
@@ -27,5 +27,5 @@ def small_reference_scene():
     group = n_op // traj.shape[1]
     op_random = np.array([[random.random(), random.random(), random.random()] for _ in range(group)])
     sc = reference_scene(args, verts, tris, traj, target, mark, op_random, cube_random)
-    sc["params"] = dict(mg.PARAMS)
+    sc["params"] = dict(mg.PARAMS_PRESS if variant == "press" else mg.PARAMS)
     return sc

@@ -14,16 +14,20 @@ from oracle.sim64 import Constants, KinematicGripper, OracleSim
 from tests.golden import make_golden as mg
 
 
-def reference_small_scene():
-    verts, tris, traj, target, mark = mg.scene_arrays()
+def reference_small_scene(variant="base"):
+    """The synthetic scene of the golden vectors as a product ClothScene;
+    variant "press" is the 300-substep scene whose grasp presses the sheet's
+    corners down (ref_fd_press_f64.npz)."""
+    verts, tris, traj, target, mark = mg.scene_arrays(variant)
+    args = mg.ARGS_PRESS if variant == "press" else mg.ARGS
     random.seed(mg.SEED_OP)
     np.random.seed(mg.SEED_CUBE)
-    n_c = mg.ARGS["rigid_cube_parameters"]["n_rigid_cube_particles"]
+    n_c = args["rigid_cube_parameters"]["n_rigid_cube_particles"]
     cube_random = np.random.rand(n_c, 3)
-    group = mg.ARGS["operator_parameters"]["n_operator_particles"] // traj.shape[1]
+    group = args["operator_parameters"]["n_operator_particles"] // traj.shape[1]
     op_random = np.array([[random.random(), random.random(), random.random()] for _ in range(group)])
-    sc = dscene.reference_scene(mg.ARGS, verts, tris, traj, target, mark, op_random, cube_random)
-    p = mg.PARAMS
+    sc = dscene.reference_scene(args, verts, tris, traj, target, mark, op_random, cube_random)
+    p = mg.PARAMS_PRESS if variant == "press" else mg.PARAMS
     sc.params.update({"E": p["E"], "nu": p["nu"], "shearing_stiffness": p["shearing_stiffness"],
                       "contact_stiffness": p["contact_stiffness"]})
     return sc

@@ -1,0 +1,126 @@
+"""FP32 CUDA path against the FP64 oracle (run on the GPU) on the benchmark
+configurations at their full sizes and horizons:
+
+  * the batched parameter sweep that bench.py times (256 cloths, 64^3 grids,
+    dt 1e-4, 300 substeps), through the bench's own path (tuned launch
+    configuration, CUDA graphs, grid tape): the stiffest, softest, smallest
+    and largest instances;
+  * the 128x128 sheet over its full 1000 substeps with checkpoints every 50;
+  * one cloth of the 64-cloth trajectory batch (64x64, 96^3, 400 substeps),
+    the gradient with respect to every per-substep gripper velocity, the
+    oracle's gradient pinned by central differences on a few coordinates.
+
+Bar: loss within 1e-5 and each gradient within 1e-4 of the FP64 value
+(relative; the velocity gradient as max-abs error over max-abs value).  Each
+check prints a "PARITY {json}" line with the measured errors."""
+import numpy as np
+import pytest
+import torch
+
+from diffcp_b200 import configs
+from tests.parity64 import COL, errors, oracle_loss_and_grads, oracle_loss_only
+
+pytestmark = pytest.mark.gpu
+
+LOSS_RTOL = 1e-5
+GRAD_RTOL = 1e-4
+PARAM_KEYS = ("E", "nu", "ks", "kc", "friction", "damping")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+
+
+def _run_batch(scenes, info, calls=2, tuned=True):
+    """Loss and gradients of every instance through the bench's path; the
+    second call restores the grids from the sized grid tape."""
+    from diffcp_b200 import autotune
+    from diffcp_b200.batch import BatchSim, ClothBatch
+    launch = (autotune.cached(scenes, info["dt"]) if tuned else None) or autotune.DEFAULT
+    b = ClothBatch(scenes, dt=info["dt"], **autotune.batch_kwargs(launch))
+    sim = BatchSim(b, n_steps=info["n_steps"], ckpt_every=info["ckpt_every"], use_graph=True, tape="auto")
+    for _ in range(calls):
+        params = b.params.clone().requires_grad_(True)
+        traj = b.traj.clone().requires_grad_(True)
+        loss = sim.loss(params, traj)
+        loss.sum().backward()
+    torch.cuda.synchronize()
+    return b, sim, loss.detach().double().cpu().numpy(), params.grad.double().cpu().numpy(), \
+        traj.grad.double().cpu().numpy()
+
+
+def _check(rec, keys=PARAM_KEYS, vel=True):
+    assert rec["loss_rel"] <= LOSS_RTOL, rec
+    for k in keys:
+        assert rec["d" + k + "_rel"] <= GRAD_RTOL, (k, rec)
+    if vel:
+        assert rec["dvel_rel_max"] <= GRAD_RTOL, rec
+
+
+def _instance(b, sim, loss, gp, gt, i, sc):
+    off, _ = b.traj_slices(i)
+    vel = gt[off: off + sc.velocities.size].reshape(sc.velocities.shape)
+    x = b.vertex_x(sim.final_state, i)
+    return float(loss[i]), {k: float(gp[i, COL[k]]) for k in PARAM_KEYS}, vel, x
+
+
+def _sweep_picks(scenes):
+    E = np.array([sc.params["E"] for sc in scenes])
+    size = np.array([sc.n_vertex for sc in scenes])
+    picks = []
+    for idx in (int(E.argmax()), int(E.argmin()), int(size.argmin()), int(size.argmax())):
+        if idx not in picks:
+            picks.append(idx)
+    return picks
+
+
+def test_parameter_sweep_instances_match_fp64_oracle():
+    scenes, info = configs.parameter_sweep(seed=0)
+    b, sim, loss, gp, gt = _run_batch(scenes, info)
+    assert (b.status() == 0).all()
+    recs = []
+    for i in _sweep_picks(scenes):
+        sc = scenes[i]
+        l32, g32, v32, x32 = _instance(b, sim, loss, gp, gt, i, sc)
+        l64, g64, v64, x64 = oracle_loss_and_grads(sc, info["n_steps"], keys=PARAM_KEYS)
+        recs.append(errors("sweep instance %d (%dx%d, E %.4g, nu %.3f, friction %.3f)" % (
+            i, int(round(np.sqrt(sc.n_vertex))), int(round(np.sqrt(sc.n_vertex))), sc.params["E"],
+            sc.params["nu"], sc.params["friction"]), l32, l64, g32, g64, v32, v64, x32, x64))
+    for rec in recs:
+        _check(rec)
+
+
+def test_large_sheet_full_horizon_matches_fp64_oracle():
+    scenes, info = configs.large_sheet(seed=0)
+    b, sim, loss, gp, gt = _run_batch(scenes, info, tuned=False)
+    assert b.status()[0] == 0
+    sc = scenes[0]
+    l32, g32, v32, x32 = _instance(b, sim, loss, gp, gt, 0, sc)
+    l64, g64, v64, x64 = oracle_loss_and_grads(sc, info["n_steps"], keys=PARAM_KEYS)
+    _check(errors("128x128 sheet, 1000 substeps, K 50", l32, l64, g32, g64, v32, v64, x32, x64))
+
+
+def test_trajectory_batch_instance_velocity_gradient_matches_fp64_oracle():
+    scenes, info = configs.trajectory_batch(seed=0)
+    b, sim, loss, gp, gt = _run_batch(scenes, info, calls=1, tuned=False)
+    assert (b.status() == 0).all()
+    sc = scenes[0]
+    l32, g32, v32, x32 = _instance(b, sim, loss, gp, gt, 0, sc)
+    l64, g64, v64, x64 = oracle_loss_and_grads(sc, info["n_steps"], keys=("E", "nu", "friction", "damping"))
+    rec = errors("trajectory batch instance 0 (64x64, 400 substeps)", l32, l64, g32, g64, v32, v64, x32, x64)
+    _check(rec, keys=("E", "nu", "friction", "damping"))
+    # the oracle's velocity gradient against central differences of its own loss
+    rng = np.random.default_rng(5)
+    scale = np.abs(v64).max()
+    for _ in range(4):
+        c = tuple(int(rng.integers(0, s)) for s in sc.velocities.shape)
+        h = 1e-4
+        vals = []
+        for sgn in (1, -1):
+            v = sc.velocities.copy()
+            v[c] += sgn * h
+            vals.append(oracle_loss_only(sc, info["n_steps"], velocities=v))
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(v64[c] - fd) <= 1e-4 * scale, (c, v64[c], fd, scale)

@@ -1,0 +1,89 @@
+"""The drop-in module (diffcp_b200.reference_api) on the reference's own scene
+(data/cloth_mesh.ply, the first grasp frames and target windows; 30 substeps
+per window), driven through compute_grad() itself, so that each window starts
+from the previous window's end state (parameter_fitting_functions.py:40-49).
+Compared with the reference source run on the same tree
+(tests/golden/ref_real_f32.npz, ref_real_fd_f64.npz): every window's loss and
+vertex history, and window 1's gradients against central differences of the
+reference's window-1 loss."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from tests.golden import make_golden as mg
+from tests.ref_tree import write_real_tree
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+MIN_SENSITIVITY = 1e-5   # see tests/test_oracle_real_scene.py
+
+
+@pytest.fixture(scope="module")
+def run(tmp_path_factory):
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    gold = np.load(os.path.join(GOLD, "ref_real_f32.npz"))
+    fd = np.load(os.path.join(GOLD, "ref_real_fd_f64.npz"))
+    import diffcp_b200.reference_api as ref
+    ref.configure(write_real_tree(tmp_path_factory.mktemp("real"), gold), seed=mg.SEED_OP, seed_cube=mg.SEED_CUBE)
+    E, nu, kc, ks = (float(x) for x in gold["params"])
+    ref.garment_E[None] = E
+    ref.garment_nu[None] = nu
+    ref.contact_stiffness[None] = kc
+    ref.shearing_stiffness[None] = ks
+    ref.initialize_objects()
+    windows = []
+    orig = ref.initialize_ti_field
+
+    def observed():
+        # compute_grad re-initialises from the window's end state here; the
+        # window's loss, gradients and history are still in place
+        windows.append({"loss": ref.loss[None], "vx": ref.vertex_x.to_numpy(),
+                        "grads": {"E": ref.garment_E.grad[None], "nu": ref.garment_nu.grad[None],
+                                  "kc": ref.contact_stiffness.grad[None], "ks": ref.shearing_stiffness.grad[None]},
+                        "seq_grad": np.array(ref.grasp_tracking_seq.grad)})
+        orig()
+
+    ref.initialize_ti_field = observed
+    try:
+        loss_mean, grads = ref.compute_grad()
+    finally:
+        ref.initialize_ti_field = orig
+    return gold, fd, windows, loss_mean
+
+
+def test_every_window_matches_reference_source(run):
+    gold, fd, windows, loss_mean = run
+    assert len(windows) == int(gold["n_windows"]) == 3
+    for g, w in enumerate(windows):
+        ref_hist = gold["w%d_vertex_x" % g]
+        assert w["vx"].shape == ref_hist.shape
+        err = np.abs(w["vx"] - ref_hist).max() / np.abs(ref_hist).max()
+        assert err < 2e-4, (g, err)
+        assert w["loss"] == pytest.approx(float(gold["w%d_loss" % g]), rel=1e-4, abs=0), g
+    assert windows[0]["loss"] == pytest.approx(float(fd["w0_loss"]), rel=2e-5, abs=0)
+    assert windows[1]["loss"] == pytest.approx(float(fd["w1_loss"]), rel=2e-5, abs=0)
+    assert loss_mean == pytest.approx(float(gold["loss_mean"]), rel=1e-4, abs=0)
+
+
+def test_window1_gradients_match_reference_finite_differences(run):
+    gold, fd, windows, _ = run
+    w = windows[1]
+    L = float(fd["w1_loss"])
+    checked = 0
+    for k, key, pv in (("E", "w1_fd_E", 0), ("nu", "w1_fd_nu", 1), ("kc", "w1_fd_contact_stiffness", 2),
+                       ("ks", "w1_fd_shearing_stiffness", 3)):
+        ref = float(fd[key])
+        if abs(ref) * float(fd["params"][pv]) / L < MIN_SENSITIVITY:
+            continue
+        assert w["grads"][k] == pytest.approx(ref, rel=1e-4, abs=0), (k, w["grads"][k], ref)
+        checked += 1
+    for name in fd.files:
+        if name.startswith("w1_fd_seq_"):
+            a, b, c = (int(t) for t in name[len("w1_fd_seq_"):].split("_"))
+            ref = float(fd[name])
+            assert ref != 0.0 and w["seq_grad"][a, b, c] == pytest.approx(ref, rel=1e-4, abs=0), name
+            checked += 1
+    assert checked >= 4

@@ -94,21 +94,43 @@ def test_svd_convention_and_clamped_backward():
     assert (np.abs(out - ref) / scale).max() < 1e-4
 
 
-def test_oracle_gradients_match_fd_of_reference_source(scene):
-    g = _load("ref_fd_f64.npz")
+def _fd_check(scene, g, window_fn, kc_material=True):
     p = {"E": float(g["params"][0]), "nu": float(g["params"][1]), "contact_stiffness": float(g["params"][2]),
          "shearing_stiffness": float(g["params"][3])}
     params = {k: v.clone().requires_grad_(True) for k, v in _params(p, torch.float64).items()}
     seq = torch.tensor(scene["grasp_point_pos"], dtype=torch.float64, requires_grad=True)
-    _, _, loss, _ = _window(scene, 0, params=params, seq=seq)
+    loss = window_fn(params, seq)
     assert float(loss) == pytest.approx(float(g["loss"]), rel=1e-12)
     loss.backward()
     for k, ref in (("E", "fd_E"), ("nu", "fd_nu"), ("kc", "fd_contact_stiffness"), ("ks", "fd_shearing_stiffness")):
         got = float(params[k].grad)
         fd = float(g[ref])
-        assert got == pytest.approx(fd, rel=2e-4, abs=1e-12), (k, got, fd)
+        if k == "kc" and not kc_material:
+            # contact (R22 < 1) barely engages in this scene: the loss moves by
+            # about 1e-9 of itself over the whole k_c range, below what a
+            # float64 central difference resolves; the press scene pins k_c
+            assert abs(fd) * p["contact_stiffness"] < 1e-9 * abs(float(g["loss"])), fd
+            continue
+        assert fd != 0.0 and got == pytest.approx(fd, rel=2e-4, abs=0), (k, got, fd)
     for name in g.files:
         if name.startswith("fd_seq_"):
             a, b, c = (int(t) for t in name[len("fd_seq_"):].split("_"))
             got = float(seq.grad[a, b, c])
-            assert got == pytest.approx(float(g[name]), rel=2e-4, abs=1e-12), (name, got, float(g[name]))
+            fd = float(g[name])
+            assert fd != 0.0 and got == pytest.approx(fd, rel=2e-4, abs=0), (name, got, fd)
+
+
+def test_oracle_gradients_match_fd_of_reference_source(scene):
+    g = _load("ref_fd_f64.npz")
+    _fd_check(scene, g, lambda params, seq: _window(scene, 0, params=params, seq=seq)[2], kc_material=False)
+
+
+def test_oracle_gradients_match_fd_of_reference_source_with_contact():
+    """The press scene (300 substeps, corners pushed down): the sheet is
+    compressed along its normal, and the contact stiffness gradient is
+    material.  Both SVD-gradient modes give the same gradients here only up
+    to the clamped adjoint's own error, so the exact mode is checked."""
+    g = _load("ref_fd_press_f64.npz")
+    sc = small_reference_scene("press")
+    assert sc["max_steps"] == int(g["max_steps"])
+    _fd_check(sc, g, lambda params, seq: _window(sc, 0, params=params, seq=seq)[2])

@@ -1,0 +1,174 @@
+"""The reference's own scene (data/cloth_mesh.ply: 427 vertices, 777
+triangles, binary float64; the first grasp frames of grasp_traj_array.npy; the
+first target windows of target_pcd_sample.npy) with a short horizon of 30
+substeps per window, against golden vectors of the reference source run on it
+(tests/golden/make_golden.py, modes real32 and real64):
+
+  * the product's PLY reader on the reference's binary file;
+  * the product's scene loader: the constants of src/initialization.py;
+  * the FP64 oracle over three grasp windows with the end-state carry-over of
+    compute_grad (parameter_fitting_functions.py:40-49): vertex histories and
+    per-window losses;
+  * the oracle's window-1 gradients against central differences of the
+    reference's window-1 loss (the carried-in state held fixed, as the Tape
+    of one window holds it).  CPU only."""
+import json
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from diffcp_b200 import io_ply, scene as dscene
+from oracle import sim64
+from oracle.scene_ref import reference_scene
+from oracle.sim64 import OracleSim
+from tests.golden import make_golden as mg
+from tests.golden import o3d_standin
+from tests.ref_tree import write_real_tree
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+# relative sensitivity |dL/dp| p / L below which a float64 central difference
+# with h = 1e-4 p cannot pin a gradient to 2e-4
+MIN_SENSITIVITY = 1e-5
+
+
+def _load(name):
+    path = os.path.join(GOLD, name)
+    if not os.path.exists(path):
+        pytest.skip("golden file %s missing" % name)
+    return np.load(path)
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return _load("ref_real_f32.npz")
+
+
+@pytest.fixture(scope="module")
+def tree(tmp_path_factory, gold):
+    return write_real_tree(tmp_path_factory.mktemp("real"), gold)
+
+
+def oracle_scene(tree):
+    """The oracle's own restatement of initialization.py on the tree, with the
+    PLY parsed by the test stand-in for open3d (not the product's reader)."""
+    with open(os.path.join(tree, "simulation_arguments.json")) as fh:
+        args = json.load(fh)
+    data = tree + args["data_dir"]
+    verts, tris = o3d_standin.read_ply_mesh(os.path.join(data, "cloth_mesh.ply"))
+    traj = np.load(os.path.join(data, "grasp_traj_array.npy"))
+    target = np.load(os.path.join(data, "target_pcd_sample.npy"))
+    mark = np.load(os.path.join(data, "rigid_cube_top_face_center_position.npy"))
+    cube_random = np.random.RandomState(mg.SEED_CUBE).rand(args["rigid_cube_parameters"]["n_rigid_cube_particles"], 3)
+    import random
+    pr = random.Random(mg.SEED_OP)
+    group = args["operator_parameters"]["n_operator_particles"] // traj.shape[1]
+    op_random = np.array([[pr.random(), pr.random(), pr.random()] for _ in range(group)])
+    return reference_scene(args, verts, tris, traj, target, mark, op_random, cube_random)
+
+
+def _params(p, grad=False):
+    names = (("E", 0), ("nu", 1), ("kc", 2), ("ks", 3))    # the golden's order: E, nu, contact, shearing
+    return {k: torch.tensor(float(p[i]), dtype=torch.float64, requires_grad=grad) for k, i in names}
+
+
+def _window(sc, g, init, params, seq):
+    """Window g from initial positions init = (vertices, operator, cube):
+    the rollout's states and the loss of compute_loss(max_steps - 2)."""
+    sim, st = OracleSim.initialize(sc["const"], init[0], sc["triangles"], init[1], init[2])
+    states = sim64.rollout(sim, st, sc["max_steps"] - 1, params, seq=seq, window=g, keep_states=True)
+    loss, _ = sim64.compute_loss(states[sc["max_steps"] - 3]["vx"],
+                                 torch.tensor(sc["targets"][g], dtype=torch.float64))
+    return states, loss
+
+
+def _end(states):
+    return tuple(states[-1][k].detach().numpy() for k in ("vx", "ox", "cx"))
+
+
+def test_product_ply_reader_reads_the_reference_binary_mesh(gold, tmp_path):
+    raw = gold["in_ply_bytes"].tobytes()
+    path = tmp_path / "cloth_mesh.ply"
+    path.write_bytes(raw)
+    v, t = io_ply.read_ply(str(path))
+    # independent parse of the layout the header declares (double x y z;
+    # list uchar uint vertex_indices)
+    body = raw[raw.index(b"end_header\n") + len(b"end_header\n"):]
+    assert b"element vertex 427" in raw and b"element face 777" in raw
+    xyz = np.frombuffer(body, dtype="<f8", count=427 * 3).reshape(427, 3)
+    faces = np.frombuffer(body, dtype=[("n", "u1"), ("i", "<u4", (3,))], count=777, offset=427 * 24)
+    assert (faces["n"] == 3).all()
+    np.testing.assert_array_equal(np.asarray(v), xyz)
+    np.testing.assert_array_equal(np.asarray(t), faces["i"].astype(np.int64))
+
+
+def test_product_scene_loader_matches_reference_constants(gold, tree):
+    sc = dscene.load_reference_scene(tree, seed=mg.SEED_OP, seed_cube=mg.SEED_CUBE)
+    for name, got in (("vertex_p_mass", sc.vertex_p_mass), ("quadrature_p_mass", sc.quadrature_p_mass),
+                      ("quadrature_p_vol", sc.quadrature_p_vol), ("operator_p_mass", sc.operator_p_mass),
+                      ("cube_p_mass", sc.cube_p_mass)):
+        assert got == pytest.approx(float(gold["const_" + name]), rel=1e-14), name
+    assert sc.meta["max_steps"] == int(gold["const_max_steps"])
+    assert sc.keyframes.shape[0] == int(gold["const_n_actions"])
+    assert sc.group_size == int(gold["const_grasper_group_size"])
+    np.testing.assert_allclose(sc.vertices, gold["soft_body_model_vertices"], rtol=0, atol=1e-15)
+    np.testing.assert_allclose(sc.keyframes, gold["grasp_point_pos"], rtol=0, atol=1e-15)
+    np.testing.assert_allclose(sc.meta["targets_by_window"], gold["target_pcd_array"], rtol=0, atol=1e-15)
+    np.testing.assert_allclose(np.asarray(sc.cube_x), gold["cube_model"], rtol=0, atol=1e-15)
+    np.testing.assert_allclose(sc.meta["operator_model"], gold["operator_model_without_position"], rtol=0,
+                               atol=1e-15)
+
+
+def test_oracle_windows_with_carry_over_match_reference_source(gold, tree):
+    sc = oracle_scene(tree)
+    n_win = int(gold["n_windows"])
+    assert n_win == 3 and sc["max_steps"] == 31
+    params = _params(gold["params"])
+    seq = torch.tensor(sc["grasp_point_pos"], dtype=torch.float64)
+    init = (sc["vertices"], sc["operator_x"], sc["cube_x"])
+    losses = []
+    for g in range(n_win):
+        states, loss = _window(sc, g, init, params, seq)
+        ref = gold["w%d_vertex_x" % g]
+        got = np.stack([s["vx"].numpy() for s in states])
+        err = np.abs(got - ref).max() / np.abs(ref).max()
+        assert err < 2e-4, (g, err)
+        np.testing.assert_allclose(states[-1]["ox"].numpy(), gold["w%d_operator_x_end" % g], rtol=0, atol=1e-5)
+        np.testing.assert_allclose(states[-1]["cx"].numpy(), gold["w%d_cube_x_end" % g], rtol=0, atol=1e-5)
+        assert float(loss) == pytest.approx(float(gold["w%d_loss" % g]), rel=1e-4, abs=0), g
+        losses.append(float(loss))
+        init = _end(states)                       # parameter_fitting_functions.py:40-49
+    assert np.mean(losses) == pytest.approx(float(gold["loss_mean"]), rel=1e-4, abs=0)
+
+
+def test_oracle_window1_gradients_match_reference_finite_differences(tree):
+    g = _load("ref_real_fd_f64.npz")
+    sc = oracle_scene(tree)
+    seq0 = torch.tensor(sc["grasp_point_pos"], dtype=torch.float64)
+    states, loss0 = _window(sc, 0, (sc["vertices"], sc["operator_x"], sc["cube_x"]), _params(g["params"]), seq0)
+    assert float(loss0) == pytest.approx(float(g["w0_loss"]), rel=1e-10, abs=0)
+    np.testing.assert_allclose(states[-1]["vx"].numpy(), g["w0_vertex_x_end"], rtol=0, atol=1e-12)
+    params = _params(g["params"], grad=True)
+    seq = seq0.clone().requires_grad_(True)
+    _, loss = _window(sc, 1, _end(states), params, seq)
+    assert float(loss) == pytest.approx(float(g["w1_loss"]), rel=1e-10, abs=0)
+    loss.backward()
+    L = float(loss)
+    checked = 0
+    for k, key, pv in (("E", "w1_fd_E", 0), ("nu", "w1_fd_nu", 1), ("kc", "w1_fd_contact_stiffness", 2),
+                       ("ks", "w1_fd_shearing_stiffness", 3)):
+        fd = float(g[key])
+        sens = abs(fd) * float(g["params"][pv]) / L
+        if sens < MIN_SENSITIVITY:
+            continue
+        got = float(params[k].grad)
+        assert got == pytest.approx(fd, rel=2e-4, abs=0), (k, got, fd)
+        checked += 1
+    for name in g.files:
+        if name.startswith("w1_fd_seq_"):
+            a, b, c = (int(t) for t in name[len("w1_fd_seq_"):].split("_"))
+            fd = float(g[name])
+            assert fd != 0.0 and float(seq.grad[a, b, c]) == pytest.approx(fd, rel=2e-4, abs=0), name
+            checked += 1
+    assert checked >= 4
