@@ -33,11 +33,11 @@ Outputs
   ref_real_f32.npz      the reference's own scene (data/cloth_mesh.ply,
                         grasp_traj_array.npy, target_pcd_sample.npy,
                         rigid_cube_top_face_center_position.npy) with a short
-                        horizon: compute_grad() itself run over 3 grasp
-                        windows of 30 substeps (end-state carry-over of
+                        horizon: compute_grad() itself run over 2 grasp
+                        windows of 300 substeps (end-state carry-over of
                         parameter_fitting_functions.py:40-49), per-window
                         losses and vertex histories, float32; and the inputs
-                        (PLY bytes, the 4 trajectory frames, the 3 target
+                        (PLY bytes, the 4 trajectory frames, the 2 target
                         windows, the arguments) so that tests rebuild the tree
   ref_real_fd_f64.npz   the same scene in float64: window 0, the carry-over,
                         and central finite differences of the window-1 loss
@@ -98,13 +98,17 @@ PARAMS = {"E": 400.0, "nu": 0.3, "contact_stiffness": 300.0, "shearing_stiffness
 ARGS_PRESS = dict(ARGS, grad_update_interval=0.0601)
 PARAMS_PRESS = {"E": 400.0, "nu": 0.3, "contact_stiffness": 1000.0, "shearing_stiffness": 150.0}
 
-# The reference's own scene with a short horizon: 30 substeps per grasp window
-# (0.00301 / 1e-4 -> max_steps 31), frames 0..3 of the grasp trajectory
-# (end_frame 3) and the first REAL_WINDOWS target windows; the other keys are
-# those of the reference's simulation_arguments.json.
-REAL_OVERRIDES = {"grad_update_interval": 0.00301, "end_frame": 3}
-REAL_WINDOWS = 3
+# The reference's own scene with a short horizon: 300 substeps per grasp
+# window (0.03001 / 1e-4 -> max_steps 301; one keyframe interval, so window g
+# moves the grippers from frame g to g + 1), frames 0..3 of the grasp
+# trajectory (end_frame 3) and the first REAL_WINDOWS target windows; the other
+# keys are those of the reference's simulation_arguments.json.  Window 1's
+# loss depends on keyframes 1 and 2 (REAL_SEQ_COORDS).
+REAL_OVERRIDES = {"grad_update_interval": 0.03001, "end_frame": 3}
+REAL_WINDOWS = 2
 REAL_FRAMES = 4
+REAL_SEQ_COORDS = ((1, 0, 1), (2, 1, 0))
+REAL_WORKERS = 6
 
 
 def write_ply(path, v, t):
@@ -326,13 +330,18 @@ def _fd_params(m, base, loss_fn, rel_h=1e-5):
     return rec
 
 
-def run_press64(tree, out):
-    m = import_reference(tree, f64=True)
-    base = dict(PARAMS_PRESS)
-    set_params(m, base)
-    rec = {"loss": window_loss(m, 0)}
-    rec.update(_fd_params(m, base, lambda: window_loss(m, 0), rel_h=1e-4))
-    for (a, b, c) in ((20, 0, 1), (40, 1, 2)):
+# Keyframe coordinates of the press scene's trajectory finite differences.  The
+# float64 run evaluates the reference's keyframe index int(f dt / interval) in
+# float64, which at substeps 73, 146, 219 and 292 picks frames 20, 40, 60, 80
+# where the reference's float32 arithmetic picks 19, 39, 59, 79; the trajectory
+# is linear, so the states do not change, but the gradients of keyframes next
+# to those boundaries (19-21, 39-41, 59-61, 79-81) do.  These are away from them.
+PRESS_SEQ_COORDS = ((10, 1, 2), (50, 0, 2))
+
+
+def press_seq_fd(m):
+    rec = {}
+    for (a, b, c) in PRESS_SEQ_COORDS:
         h = 1e-6
         vals = []
         for sgn in (1, -1):
@@ -340,6 +349,16 @@ def run_press64(tree, out):
             vals.append(window_loss(m, 0))
             m.grasp_point_pos[a, b, c] -= sgn * h
         rec["fd_seq_%d_%d_%d" % (a, b, c)] = (vals[0] - vals[1]) / (2 * h)
+    return rec
+
+
+def run_press64(tree, out):
+    m = import_reference(tree, f64=True)
+    base = dict(PARAMS_PRESS)
+    set_params(m, base)
+    rec = {"loss": window_loss(m, 0)}
+    rec.update(_fd_params(m, base, lambda: window_loss(m, 0), rel_h=1e-4))
+    rec.update(press_seq_fd(m))
     rec["params"] = np.array([base["E"], base["nu"], base["contact_stiffness"], base["shearing_stiffness"]])
     rec["max_steps"] = np.array(m.max_steps)
     np.savez_compressed(out, **rec)
@@ -402,10 +421,50 @@ def run_real32(tree, out):
     np.savez_compressed(out, **rec)
 
 
+_REAL64 = {}
+
+
+def _real64_worker(tree, carried_path):
+    """Process initialiser: the reference in float64 and window 0's end state."""
+    m = import_reference(tree, f64=True)
+    m.initialize_objects()          # the keyframes (grasp_tracking_seq), as in the parent process
+    c = np.load(carried_path)
+    _REAL64.update(m=m, carried={k: c[k] for k in c.files})
+
+
+def _window1_loss(m, carried, params, seq_delta=None):
+    """compute_grad's window 1 (parameter_fitting_functions.py:21-29) from the
+    carried-in state of window 0 (lines 40-49), with ``params`` and, when
+    ``seq_delta`` = ((a, b, c), h), keyframe (a, b, c) moved by h."""
+    set_params(m, params)
+    m.initial_operator_x.from_numpy(carried["op"])
+    m.initial_vertex_x.from_numpy(carried["vx"])
+    m.lagrangian_mesh_element.from_numpy(carried["faces"])
+    m.initial_cube_x.from_numpy(carried["cube"])
+    m.initialize_ti_field()
+    if seq_delta is not None:
+        (a, b, c), h = seq_delta
+        m.grasp_tracking_seq[a][b, c] += h
+    try:
+        return window_loss_carry(m, 1)
+    finally:
+        if seq_delta is not None:
+            m.grasp_tracking_seq[a][b, c] -= h
+
+
+def _real64_task(task):
+    m, carried = _REAL64["m"], _REAL64["carried"]
+    params, seq_delta = task
+    return _window1_loss(m, carried, params, seq_delta)
+
+
 def run_real64(tree, out):
     """Window 0, the carry-over of compute_grad (parameter_fitting_functions.py:
     40-49), and central differences of the window-1 loss with the carried-in
-    state held fixed, in float64."""
+    state held fixed, in float64.  The window-1 evaluations run in parallel
+    processes, each with its own copy of the reference's module state."""
+    import concurrent.futures
+    import multiprocessing
     m = import_reference(tree, f64=True)
     base = _real_initial_params(m)
     set_params(m, base)
@@ -413,29 +472,37 @@ def run_real64(tree, out):
     rec = {"w0_loss": window_loss_carry(m, 0)}
     last = m.max_steps - 1
     carried = {"op": m.operator_x.to_numpy()[last], "vx": m.vertex_x.to_numpy()[last],
-               "cube": m.cube_x.to_numpy()[last]}
-    faces = np.asarray(m.soft_body_mesh.triangles)
+               "cube": m.cube_x.to_numpy()[last], "faces": np.asarray(m.soft_body_mesh.triangles)}
     rec["w0_vertex_x_end"] = carried["vx"]
-
-    def window1():
-        m.initial_operator_x.from_numpy(carried["op"])
-        m.initial_vertex_x.from_numpy(carried["vx"])
-        m.lagrangian_mesh_element.from_numpy(faces)
-        m.initial_cube_x.from_numpy(carried["cube"])
-        m.initialize_ti_field()
-        return window_loss_carry(m, 1)
-
-    rec["w1_loss"] = window1()
-    rec.update({"w1_" + k: v for k, v in _fd_params(m, base, window1, rel_h=1e-4).items()})
-    for (a, b, c) in ((0, 0, 1), (1, 1, 0)):
-        h = 1e-7
-        vals = []
+    carried_path = out + ".carried.npz"
+    np.savez(carried_path, **carried)
+    tasks, keys = [(dict(base), None)], ["w1_loss"]
+    rel_h = 1e-4
+    for name in ("E", "nu", "contact_stiffness", "shearing_stiffness"):
         for sgn in (1, -1):
-            m.grasp_tracking_seq[a][b, c] += sgn * h     # the keyframes of this window (set by initialize_objects)
-            vals.append(window1())
-            m.grasp_tracking_seq[a][b, c] -= sgn * h
-        rec["w1_fd_seq_%d_%d_%d" % (a, b, c)] = (vals[0] - vals[1]) / (2 * h)
+            p = dict(base)
+            p[name] = base[name] + sgn * rel_h * base[name]
+            tasks.append((p, None))
+            keys.append(("param", name, sgn))
+    h_seq = 1e-7
+    for coord in REAL_SEQ_COORDS:
+        for sgn in (1, -1):
+            tasks.append((dict(base), (coord, sgn * h_seq)))
+            keys.append(("seq", coord, sgn))
+    ctx = multiprocessing.get_context("spawn")
+    with concurrent.futures.ProcessPoolExecutor(REAL_WORKERS, mp_context=ctx, initializer=_real64_worker,
+                                                initargs=(tree, carried_path)) as ex:
+        vals = list(ex.map(_real64_task, tasks))
+    os.remove(carried_path)
+    rec["w1_loss"] = vals[0]
+    res = dict(zip(keys[1:], vals[1:]))
+    for name in ("E", "nu", "contact_stiffness", "shearing_stiffness"):
+        h = rel_h * base[name]
+        rec["w1_fd_" + name] = (res[("param", name, 1)] - res[("param", name, -1)]) / (2 * h)
+    for coord in REAL_SEQ_COORDS:
+        rec["w1_fd_seq_%d_%d_%d" % coord] = (res[("seq", coord, 1)] - res[("seq", coord, -1)]) / (2 * h_seq)
     rec["params"] = np.array([base["E"], base["nu"], base["contact_stiffness"], base["shearing_stiffness"]])
+    rec["max_steps"] = np.array(m.max_steps)
     np.savez_compressed(out, **rec)
 
 
