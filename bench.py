@@ -40,16 +40,17 @@ sys.path.insert(0, ROOT)
 METRIC = "fwd+bwd particle-steps/s"
 UNIT = "particle-steps/s"
 # Algorithmic bytes per particle of one launch (float32 state, grid traffic
-# excluded), for each kernel of the substep and its adjoint; see DESIGN.md.
+# excluded), for each kernel of the substep and its adjoint: the particle
+# state, rest data and per-vertex sums the kernel must read or write once.
 KERNEL_BYTES = {
-    "k_tri_forward": {"tri": 252},
+    "k_tri_forward": {"tri": 228},
     "k_point_p2g": {"vertex": 88},
     "k_grid": {"node": 48},
-    "k_g2p": {"vertex": 84, "tri": 156},
-    "k_g2p_adj": {"vertex": 96, "tri": 180},
+    "k_g2p": {"vertex": 84, "tri": 204},
+    "k_g2p_adj": {"vertex": 96, "tri": 144},
     "k_grid_adj": {"node": 64},
     "k_point_adj": {"vertex": 156},
-    "k_tri_adj": {"tri": 396},
+    "k_tri_adj": {"tri": 372},
     "k_vertex_collect": {"vertex": 112},
 }
 # Whole fwd+bwd substep, per particle (float32): vertex 420 B, triangle 1068 B.
@@ -151,66 +152,99 @@ def counts(scenes):
 
 
 # ------------------------------------------------------------------ CPU
-def cpu_rate(scenes, info, seconds=15.0, steps=1, warmup=0):
+def median_instance(scenes):
+    sizes = [s.n_vertex + s.n_tri for s in scenes]
+    i = int(np.argsort(sizes)[len(sizes) // 2])
+    return i, scenes[i]
+
+
+def cpu_rate(scenes, info, seconds=15.0, steps=1, warmup=0, min_substeps=20):
     """Oracle (torch, float32, all host threads) fwd+bwd rate on a bounded
-    sample of the workload: the instance nearest the median size; each of
-    ``steps`` timed steps runs as many substeps as fit in about
-    ``seconds / steps`` (after ``warmup`` short untimed steps)."""
+    sample of the workload: the instance nearest the median size.  Each of
+    ``steps`` timed steps is the forward and adjoint of ``n`` substeps of it,
+    n >= ``min_substeps`` sized so that the timed steps take about
+    ``seconds``; the oracle's set-up (rest frames, state 0) is outside the
+    timed region, as the GPU arm's is."""
     import torch
     from oracle import sim64
     from oracle.sim64 import Constants, KinematicGripper, OracleSim
-    sizes = [s.n_vertex + s.n_tri for s in scenes]
-    sc = scenes[int(np.argsort(sizes)[len(sizes) // 2])]
+    idx, sc = median_instance(scenes)
     dt = info["dt"]
     d = torch.float32
     const = Constants(n_grid=sc.n_grid, dt=dt, vertex_p_mass=sc.vertex_p_mass, quadrature_p_mass=sc.quadrature_p_mass,
                       quadrature_p_vol=sc.quadrature_p_vol, gravity_dv=sc.gravity_dv, bound=sc.bound)
+    targets = torch.tensor(sc.targets, dtype=d)
 
-    def run(n):
+    def setup():
         osim, st = OracleSim.initialize(const, sc.vertices, sc.triangles, dtype=d)
         p = {k: torch.tensor(float(v), dtype=d, requires_grad=True) for k, v in
              zip(("E", "nu", "ks", "kc", "friction", "damping"), sc.param_row())}
         vel = torch.tensor(sc.velocities, dtype=d, requires_grad=True)
         grip = KinematicGripper(sc.gripper_radius, torch.tensor(sc.centers, dtype=d), vel)
+        return osim, st, p, grip
+
+    def run(n, ready):
+        osim, st, p, grip = ready
         for f in range(n):
             st = osim.substep(st, f, 0, p, friction=p["friction"], damping=p["damping"], grip=grip)
-        lo, _ = sim64.compute_loss(st["vx"], torch.tensor(sc.targets, dtype=d))
+        lo, _ = sim64.compute_loss(st["vx"], targets)
         lo.backward()
 
+    ready = setup()
     t0 = time.perf_counter()
-    run(2)
+    run(2, ready)
     per = (time.perf_counter() - t0) / 2
-    # one step = fwd+bwd of n substeps, n sized so that the timed steps take about `seconds`
-    n = int(max(2, min(info["n_steps"], seconds / max(steps, 1) / max(per, 1e-3))))
+    n = int(max(min_substeps, min(info["n_steps"], seconds / max(steps, 1) / max(per, 1e-3))))
     for _ in range(warmup):
-        run(2)
-    t0 = time.perf_counter()
-    for _ in range(max(steps, 1)):
-        run(n)
-    el = time.perf_counter() - t0
+        run(2, setup())
+    el = 0.0
     k = max(steps, 1)
+    for _ in range(k):
+        ready = setup()
+        t0 = time.perf_counter()
+        run(n, ready)
+        el += time.perf_counter() - t0
     rate = (sc.n_vertex + sc.n_tri) * n * k / el
     return {"value": rate, "unit": UNIT, "cores": torch.get_num_threads(), "kind": "port",
-            "ms_per_step": 1e3 * el / k,
-            "sample": "CPU oracle (torch float32) fwd+bwd of %d substeps of one %d-vertex/%d-triangle cloth of the "
-                      "workload per step, %d step(s) in %.1f s" % (n, sc.n_vertex, sc.n_tri, k, el)}
+            "ms_per_step": 1e3 * el / k, "instance": idx, "substeps_per_step": n,
+            "sample": "CPU oracle port (torch float32, %d threads; the reference's Taichi is not installed) fwd+bwd "
+                      "of %d substeps of instance %d of the workload (%d vertices + %d triangles, the median size) "
+                      "per step, %d timed step(s) in %.1f s, set-up outside the timed region" % (
+                          torch.get_num_threads(), n, idx, sc.n_vertex, sc.n_tri, k, el)}
+
+
+def workload_config(scenes, info, world=1):
+    """The `config` of the JSON line, the same for both arms: what the
+    workload is, not how a run executed it."""
+    from diffcp_b200.batch import POINT_STATE, TRI_STATE
+    nv, nt = counts(scenes)
+    state_floats = POINT_STATE * nv + TRI_STATE * nt
+    return {"workload": info["desc"], "instances": len(scenes), "vertices": nv, "triangles": nt,
+            "substeps": info["n_steps"], "checkpoint_every": info["ckpt_every"],
+            "l2": "inputs larger than L2 (one state snapshot is %.0f MB; every substep reads its own)"
+                  % (state_floats * 4 / 1e6),
+            "parallelism": "independent instances per rank" if world > 1 else "one GPU"}
 
 
 def profile_substeps(args):
     """Two eager rollouts of ``args.profile_substeps`` substeps of the workload
-    (forward, Chamfer, adjoint) through the same path as the bench: the first
-    sizes the grid tape, the second restores from it and reads the next
-    state's C in the adjoint.  A few GB on the device; for kernel profilers.
-    Launch order of the second rollout, per substep: forward k_tri_forward,
-    k_point_p2g, k_tape_reserve, k_grid, k_g2p x2; adjoint k_tape_restore,
-    k_tri_forward and k_point_p2g (both return at once), k_grid, k_g2p_adj,
-    k_grid_adj, k_point_adj, k_tri_adj (and k_vertex_collect after substep 0)."""
+    (or of its first ``args.profile_instances`` instances) with forward,
+    Chamfer and adjoint, through the same path as the bench: the first sizes
+    the grid tape, the second records into it and the adjoint reads it.  A few
+    GB on the device at most; for kernel profilers.  Launch order of the second
+    rollout, per substep: forward k_tri_forward, k_point_p2g, k_tape_reserve,
+    k_grid, k_g2p (points, then triangles); adjoint k_tri_forward and
+    k_point_p2g (both return at once), k_grid, k_g2p_adj, k_grid_adj,
+    k_point_adj, k_tri_adj (and k_vertex_collect after substep 0)."""
     import torch
     from diffcp_b200 import autotune
     from diffcp_b200.batch import BatchSim, ClothBatch
     scenes, info = workload(args.workload, 0)
     cache = args.tune_cache or autotune.CACHE
+    # the launch configuration tuned for the whole workload, also on a slice of it
     launch = (autotune.cached(scenes, info["dt"], cache=cache) if os.path.exists(cache) else None) or autotune.DEFAULT
+    if args.profile_instances:
+        scenes = scenes[: args.profile_instances]
     b = ClothBatch(scenes, dt=info["dt"], **autotune.batch_kwargs(launch))
     n = args.profile_substeps
     sim = BatchSim(b, n_steps=n, ckpt_every=1, use_graph=False, tape="auto")
@@ -236,6 +270,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-substeps", type=int, default=0,
                     help="run this many eager forward + adjoint substeps of the workload and exit (for ncu)")
+    ap.add_argument("--profile-instances", type=int, default=0,
+                    help="with --profile-substeps: only the first this many instances of the workload")
     ap.add_argument("--tune", action="store_true", help="autotune the launch configuration before timing")
     ap.add_argument("--tune-cache", default=None, help="autotuner cache file (default diffcp_b200/tuned.json)")
     ap.add_argument("--no-single", action="store_true", help="skip the single-instance plain-launch measurement")
@@ -253,7 +289,7 @@ def main():
         line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-                "config": {"workload": info["desc"]}, "cpu_baseline": cb,
+                "config": workload_config(scenes, info, args.gpus), "cpu_baseline": cb,
                 "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -390,8 +426,7 @@ def main():
     # ---- the same work as single instances with plain per-kernel launches (no CUDA graph)
     single = None
     if not args.no_single and len(scenes) > 1:
-        sizes = [s_.n_vertex + s_.n_tri for s_ in scenes]
-        sc1 = scenes[int(np.argsort(sizes)[len(sizes) // 2])]
+        _, sc1 = median_instance(scenes)
         b1 = ClothBatch([sc1], dt=info["dt"], device=dev, **autotune.batch_kwargs(launch))
         sim1 = BatchSim(b1, n_steps=info["n_steps"], ckpt_every=info["ckpt_every"], use_graph=False, tape=tape)
         p1 = b1.params.clone().requires_grad_(True)
@@ -422,13 +457,9 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": info["desc"], "instances": len(scenes), "vertices": nv, "triangles": nt,
-                   "substeps": info["n_steps"], "checkpoint_every": info["ckpt_every"],
-                   "l2": "inputs larger than L2 (state snapshot %.0f MB, rollout buffer %.1f GB)"
-                         % (batch.S * 4 / 1e6, sim._buf.numel() * 4 / 1e9),
-                   "parallelism": "independent instances per rank" if world > 1 else "one GPU",
-                   "launch": launch, "grid_tape": tape_info,
-                   "peak_device_bytes": int(torch.cuda.max_memory_allocated(dev))},
+        "config": workload_config(scenes, info, world),
+        "run": {"launch": launch, "grid_tape": tape_info, "rollout_buffer_gb": sim._buf.numel() * 4 / 1e9,
+                "peak_device_bytes": int(torch.cuda.max_memory_allocated(dev))},
         "roofline": roof,
         "step_roofline": {"achieved": step_alg / (ms_max / 1e3) / 1e9, "unit": "GB/s", "peak": peak,
                           "frac": step_alg / (ms_max / 1e3) / 1e9 / peak,

@@ -16,6 +16,9 @@ from .native import DcpInstance, DcpOptions, DcpSizes, check
 from .scene import ClothScene, morton_order
 
 PRM_STRIDE = 8
+# Floats per particle in a state snapshot (vertex / operator / cube, triangle)
+# and per triangle in the rest buffer (include/diffcp_b200.h).
+POINT_STATE, TRI_STATE, TRI_REST = 15, 18, 21
 
 
 def _ptr(t: Optional[torch.Tensor]) -> Optional[int]:
@@ -161,7 +164,7 @@ class ClothBatch:
 
     def rest_x0(self) -> torch.Tensor:
         """[3][Nv] rest vertex positions held in the rest buffer."""
-        o = 12 * self.nt
+        o = TRI_REST * self.nt
         return self.rest[o: o + 3 * self.nv].view(3, self.nv)
 
     def rest_n0(self) -> torch.Tensor:
@@ -170,7 +173,7 @@ class ClothBatch:
     def absolute_fields(self, state: torch.Tensor):
         """Like :meth:`state_fields` with positions and d3 made absolute."""
         f = dict(self.state_fields(state))
-        o = 12 * self.nt + 3 * self.nv
+        o = TRI_REST * self.nt + 3 * self.nv
         f["vx"] = f["vx"] + self.rest_x0()
         f["qd3"] = f["qd3"] + self.rest_n0()
         f["ox"] = f["ox"] + self.rest[o: o + 3 * self.no].view(3, self.no)
@@ -180,15 +183,18 @@ class ClothBatch:
 
     def state_fields(self, state: torch.Tensor):
         """Dict of component-major views of one state snapshot (positions are
-        displacements from the rest configuration, 'qd3' is d3 - n0)."""
+        displacements from the rest configuration, 'qd3' is d3 - n0; 'qx',
+        'qv' the triangles' centroid position (absolute) and velocity)."""
         nv, nt, no, nc = self.nv, self.nt, self.no, self.nc
-        v = state[: 15 * nv].view(15, nv)
-        t = state[15 * nv: 15 * nv + 12 * nt].view(12, nt)
-        o0 = 15 * nv + 12 * nt
-        o = state[o0: o0 + 15 * no].view(15, no)
-        c = state[o0 + 15 * no: o0 + 15 * no + 15 * nc].view(15, nc)
-        return {"vx": v[0:3], "vv": v[3:6], "vC": v[6:15], "qC": t[0:9], "qd3": t[9:12], "ox": o[0:3],
-                "ov": o[3:6], "oC": o[6:15], "cx": c[0:3], "cv": c[3:6], "cC": c[6:15]}
+        P, T = POINT_STATE, TRI_STATE
+        v = state[: P * nv].view(P, nv)
+        t = state[P * nv: P * nv + T * nt].view(T, nt)
+        o0 = P * nv + T * nt
+        o = state[o0: o0 + P * no].view(P, no)
+        c = state[o0 + P * no: o0 + P * no + P * nc].view(P, nc)
+        return {"vx": v[0:3], "vv": v[3:6], "vC": v[6:15], "qC": t[0:9], "qd3": t[9:12], "qx": t[12:15],
+                "qv": t[15:18], "ox": o[0:3], "ov": o[3:6], "oC": o[6:15], "cx": c[0:3], "cv": c[3:6],
+                "cC": c[6:15]}
 
     def save_rest(self):
         """Copies of the rest positions (vertices, operator, cube)."""

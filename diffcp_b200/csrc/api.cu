@@ -178,8 +178,8 @@ struct DcpBatch {
 
 static void fill_sizes(const Layout& L, int n, DcpSizes* s) {
   s->n_vertex = L.nv; s->n_tri = L.nt; s->n_operator = L.no; s->n_cube = L.nc; s->n_target = L.nq;
-  s->state_floats = 15 * (L.nv + L.no + L.nc) + 12 * L.nt;
-  s->rest_floats = 12 * L.nt + 3 * (L.nv + L.no + L.nc);
+  s->state_floats = kPointState * (L.nv + L.no + L.nc) + kTriState * L.nt;
+  s->rest_floats = kTriRest * L.nt + 3 * (L.nv + L.no + L.nc);
   s->traj_floats = L.traj;
   s->param_floats = (long long)PRM_STRIDE * n;
   s->static_bytes = (long long)L.static_bytes;
@@ -280,7 +280,17 @@ int dcp_create(const DcpInstance* inst, int32_t n_inst, const DcpOptions* opt, c
   B.total_nodes = L.total_nodes;
   B.total_blocks = L.total_nodes / 64;
   b->L.block = opt->chunk;
-  b->L.grid_ctas = opt->grid_ctas > 0 ? opt->grid_ctas : 148 * 8;
+  // streaming multiprocessors of the current device: the grid-stride kernels
+  // launch a multiple of this count
+  int dev = 0, sms = 0;
+  e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess || sms <= 0) {
+    delete b;
+    return cuda_fail(e != cudaSuccess ? e : cudaErrorInvalidValue, "dcp_create: multiprocessor count");
+  }
+  b->L.sm_count = sms;
+  b->L.grid_ctas = opt->grid_ctas > 0 ? opt->grid_ctas : sms * 8;
   const int default_minb[3] = {2, 2, 1};
   for (int k = 0; k < 3; ++k) b->L.min_blocks[k] = opt->min_blocks[k] > 0 ? opt->min_blocks[k] : default_minb[k];
   b->L.prof = &b->prof;

@@ -3,11 +3,17 @@
 //
 // HBM layout (all instances concatenated, structure of arrays):
 //   state snapshot   [15][Nv] vertex  u(3) v(3) C(9)    u = x - x0 (displacement)
-//                    [12][Nt] triangle C(9) delta3(3)   delta3 = d3 - n0
+//                    [18][Nt] triangle C(9) delta3(3) xc(3) vc(3)
+//                             delta3 = d3 - n0; xc, vc the centroid position
+//                             (absolute) and velocity, kept so that the
+//                             triangle kernels read them coalesced instead of
+//                             gathering three vertices
 //                    [15][No] operator u v C
 //                    [15][Nc] cube     u v C
-//   rest             [9][Nt] D0^-1, [3][Nt] n0 (rest normal), [3][Nv], [3][No],
-//                    [3][Nc] rest positions x0
+//   rest             [9][Nt] D0^-1, [3][Nt] n0 (rest normal), [6][Nt] rest
+//                    edges e1 = x0b - x0a, e2 = x0c - x0a (D0's first two
+//                    columns), [3][Nt] rest centroid, [3][Nv], [3][No], [3][Nc]
+//                    rest positions x0
 // Positions and the triangle's third column are stored relative to the rest
 // configuration so that float32 keeps the small strains that drive the stress
 // (absolute positions near 0.5 would leave ~1e-5 strain resolution).
@@ -77,6 +83,11 @@ struct BatchDev {
   long long total_nodes, total_blocks;
 };
 
+// Floats per particle of a state snapshot and of the rest buffer.
+constexpr int kPointState = 15, kTriState = 18, kTriRest = 21;
+// Rows of a triangle's state: C 0-8, delta3 9-11, centroid 12-14, its velocity 15-17.
+enum { TRI_C = 0, TRI_D3 = 9, TRI_XC = 12, TRI_VC = 15 };
+
 struct StateP {
   float* v;
   float* t;
@@ -86,9 +97,9 @@ struct StateP {
 __host__ __device__ inline StateP state_ptrs(float* base, int nv, int nt, int no) {
   StateP s;
   s.v = base;
-  s.t = base + 15LL * nv;
-  s.o = s.t + 12LL * nt;
-  s.c = s.o + 15LL * no;
+  s.t = base + (long long)kPointState * nv;
+  s.o = s.t + (long long)kTriState * nt;
+  s.c = s.o + (long long)kPointState * no;
   return s;
 }
 
@@ -109,6 +120,8 @@ struct TapeP {
 struct RestP {
   const float* Di;  // [9][nt]
   const float* n0;  // [3][nt]
+  const float* e;   // [6][nt] rest edges e1 (rows 0-2), e2 (rows 3-5)
+  const float* tc;  // [3][nt] rest centroid
   const float* xv;  // [3][nv]
   const float* xo;  // [3][no]
   const float* xc;  // [3][nc]
@@ -117,7 +130,9 @@ __host__ __device__ inline RestP rest_ptrs(const float* rest, int nv, int nt, in
   RestP r;
   r.Di = rest;
   r.n0 = rest + 9LL * nt;
-  r.xv = rest + 12LL * nt;
+  r.e = rest + 12LL * nt;
+  r.tc = rest + 18LL * nt;
+  r.xv = rest + (long long)kTriRest * nt;
   r.xo = r.xv + 3LL * nv;
   r.xc = r.xo + 3LL * no;
   return r;

@@ -22,8 +22,9 @@
 // Reverse substep: k_g2p_adj, k_grid_adj, k_point_adj, k_tri_adj; k_vertex_collect
 // after a single substep or after a rollout's last one (inside a rollout the
 // next substep's k_g2p_adj takes in the triangles' per-vertex adjoint sums).
-// Grid tape (optional): k_tape_reserve / k_tape_restore keep each forward
-// substep's particle-to-grid result so that the reverse substep skips P2G.
+// Grid tape (optional): k_tape_reserve and k_grid keep each forward
+// substep's particle-to-grid result; the reverse substep's k_grid and
+// k_grid_adj read it in place and its P2G launches return at once.
 // Replay (forward only, simulation_without_grad.py): k_reset_tri /
 // k_reset_vertex re-base the rest frames every few substeps.
 #include <cuda_runtime.h>
@@ -98,62 +99,75 @@ __global__ void k_init(BatchDev B, const float* __restrict__ x0v, const float* _
     const float pc[3] = {x0v[c], x0v[nv + c], x0v[2 * nv + c]};
     float inv[9], nrm[3];
     rest_frame(pa, pb, pc, inv, nrm);
+    const long long nt = B.nt;
     float* Di = const_cast<float*>(R.Di);
     float* n0 = const_cast<float*>(R.n0);
-    for (int q = 0; q < 9; ++q) Di[q * (long long)B.nt + t] = inv[q];
-    for (int q = 0; q < 12; ++q) S.t[q * (long long)B.nt + t] = 0.f;
-    for (int q = 0; q < 3; ++q) n0[q * (long long)B.nt + t] = nrm[q];
+    float* e = const_cast<float*>(R.e);
+    float* tc = const_cast<float*>(R.tc);
+    for (int q = 0; q < 9; ++q) Di[q * nt + t] = inv[q];
+    for (int q = 0; q < TRI_XC; ++q) S.t[q * nt + t] = 0.f;
+    const float third = 1.f / 3.f;
+    for (int a = 0; a < 3; ++a) {
+      n0[a * nt + t] = nrm[a];
+      e[a * nt + t] = pb[a] - pa[a];
+      e[(3 + a) * nt + t] = pc[a] - pa[a];
+      const float c = third * ((pa[a] + pb[a]) + pc[a]);
+      tc[a * nt + t] = c;                       // the centroid is the rest centroid at rest
+      S.t[(TRI_XC + a) * nt + t] = c;
+      S.t[(TRI_VC + a) * nt + t] = 0.f;
+    }
   }
 }
 
-// Triangle geometry at one state: vertex ids, rest positions, displacements,
-// absolute positions, velocities, centroid.
+// Triangle geometry at one state: vertex ids and displacements of the three
+// corners (scattered loads), centroid position and velocity (kept in the
+// state: coalesced loads).
 struct TriGeom {
   int vid[3];
-  float X0[3][3];  // [corner][axis]
-  float U[3][3];
-  float V[3][3];
+  float U[3][3];  // [corner][axis]
   float xc[3], vc[3];
 };
-__device__ __forceinline__ void load_tri(const BatchDev& B, const StateP& S, const RestP& R, long long t, bool need_v,
-                                         TriGeom& g) {
-  const long long nv = B.nv, nt = B.nt;
+__device__ __forceinline__ void load_tri_ids(const BatchDev& B, long long t, int vid[3]) {
+  const long long nt = B.nt;
 #pragma unroll
-  for (int c = 0; c < 3; ++c) g.vid[c] = __ldg(B.tri_v + c * nt + t);
+  for (int c = 0; c < 3; ++c) vid[c] = __ldg(B.tri_v + c * nt + t);
+}
+__device__ __forceinline__ void load_centroid(const BatchDev& B, const StateP& S, long long t, bool need_v, TriGeom& g) {
+  const long long nt = B.nt;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    g.xc[a] = __ldg(S.t + (TRI_XC + a) * nt + t);
+    g.vc[a] = need_v ? __ldg(S.t + (TRI_VC + a) * nt + t) : 0.f;
+  }
+}
+__device__ __forceinline__ void load_corner_u(const BatchDev& B, const StateP& S, long long t, TriGeom& g) {
+  const long long nv = B.nv;
+  load_tri_ids(B, t, g.vid);
 #pragma unroll
   for (int c = 0; c < 3; ++c)
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      g.X0[c][a] = __ldg(R.xv + a * nv + g.vid[c]);
-      g.U[c][a] = __ldg(S.v + a * nv + g.vid[c]);
-    }
-  const float third = 1.f / 3.f;
+    for (int a = 0; a < 3; ++a) g.U[c][a] = __ldg(S.v + a * nv + g.vid[c]);
+}
+__device__ __forceinline__ void load_rest_edges(const BatchDev& B, const RestP& R, long long t, float e[6]) {
+  const long long nt = B.nt;
 #pragma unroll
-  for (int a = 0; a < 3; ++a)
-    g.xc[a] = third * (((g.X0[0][a] + g.U[0][a]) + (g.X0[1][a] + g.U[1][a])) + (g.X0[2][a] + g.U[2][a]));
-  if (need_v) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-      for (int a = 0; a < 3; ++a) g.V[c][a] = __ldg(S.v + (3 + a) * nv + g.vid[c]);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) g.vc[a] = third * ((g.V[0][a] + g.V[1][a]) + g.V[2][a]);
-  }
+  for (int q = 0; q < 6; ++q) e[q] = __ldg(R.e + q * nt + t);
 }
 
 // d = [x2 - x1, x3 - x1, d3] and F = d D0^-1 (simulation.py:395-407), returned
 // as the deviation Fe = F - I = (d - D0) D0^-1 with d - D0 formed from
-// displacements and delta3 = d3 - n0.
-__device__ __forceinline__ void tri_F(const TriGeom& g, const float dl3[3], const float n0[3], const float Di[9],
-                                      M3<float>& d, M3<float>& Fe) {
+// displacements and delta3 = d3 - n0; e holds D0's first two columns (the
+// rest edges).
+__device__ __forceinline__ void tri_F(const TriGeom& g, const float e[6], const float dl3[3], const float n0[3],
+                                      const float Di[9], M3<float>& d, M3<float>& Fe) {
   float dd[9];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     dd[3 * a + 0] = g.U[1][a] - g.U[0][a];
     dd[3 * a + 1] = g.U[2][a] - g.U[0][a];
     dd[3 * a + 2] = dl3[a];
-    d.m[3 * a + 0] = (g.X0[1][a] - g.X0[0][a]) + dd[3 * a + 0];
-    d.m[3 * a + 1] = (g.X0[2][a] - g.X0[0][a]) + dd[3 * a + 1];
+    d.m[3 * a + 0] = e[a] + dd[3 * a + 0];
+    d.m[3 * a + 1] = e[3 + a] + dd[3 * a + 1];
     d.m[3 * a + 2] = n0[a] + dl3[a];
   }
 #pragma unroll
@@ -168,7 +182,7 @@ __device__ __forceinline__ void load_tri_rest(const BatchDev& B, const RestP& R,
   const long long nt = B.nt;
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
-    dl3[q] = __ldg(S.t + (9 + q) * nt + t);
+    dl3[q] = __ldg(S.t + (TRI_D3 + q) * nt + t);
     n0[q] = __ldg(R.n0 + q * nt + t);
   }
 #pragma unroll
@@ -205,19 +219,21 @@ __device__ __forceinline__ void tri_forward_chunk(const BatchDev& B, const float
     float A[9];
     // the triangle's own (coalesced) loads first, so that their latency
     // overlaps the dependent vertex gathers of load_tri
-    float dl3[3], n0[3], Di[9];
+    float dl3[3], n0[3], Di[9], e[6];
 #pragma unroll
     for (int q = 0; q < 9; ++q) A[q] = __ldg(S.t + q * nt + t) * m;
     load_tri_rest(B, R, S, t, dl3, n0, Di);
+    load_rest_edges(B, R, t, e);
     TriGeom g;
-    load_tri(B, S, R, t, true, g);
+    load_centroid(B, S, t, true, g);
+    load_corner_u(B, S, t, g);
     make_stencil(g.xc, I, st, B.status, ch.inst);
     const float* prm = params + ch.inst * PRM_STRIDE;
     float mu, la;
     lame(prm[PRM_E], prm[PRM_NU], mu, la);
     const float ks = prm[PRM_KS], kc = prm[PRM_KC];
     M3<float> d, Fe;
-    tri_F(g, dl3, n0, Di, d, Fe);
+    tri_F(g, e, dl3, n0, Di, d, Fe);
     if (fdev) {  // stress from the F kept across a rest-frame reset (replay)
 #pragma unroll
       for (int q = 0; q < 9; ++q) Fe.m[q] = __ldg(fdev + q * nt + t);
@@ -409,18 +425,26 @@ __device__ __forceinline__ int kinematic_hit(const InstDev& I, const float* traj
   return hit;
 }
 
+// GRID_FORWARD: records the (p, m) of this substep into the tape when the tape
+// reserved it room.  GRID_RECOMPUTE (adjoint substep): when the tape holds this
+// substep's P2G result, reads the active blocks and their (p, m) from the tape
+// in place; otherwise from the P2G this substep recomputed.
 __global__ void __launch_bounds__(256) k_grid(BatchDev B, const float* __restrict__ params,
                                               const float* __restrict__ traj, int step, int mode, TapeP T) {
-  const int count = B.counters[0];
-  const int tape_at = T.meta ? T.meta[step].x : -1;
+  const int2 tm = T.meta ? T.meta[step] : make_int2(-1, 0);
+  const bool from_tape = mode == GRID_RECOMPUTE && tm.x >= 0;
+  const int count = from_tape ? tm.y : B.counters[0];
+  const int record_at = mode == GRID_FORWARD ? tm.x : -1;
   const int per = blockDim.x >> 6, l = threadIdx.x & 63;
   for (int item = blockIdx.x * per + (threadIdx.x >> 6); item < count; item += gridDim.x * per) {
-    const int blk = B.list_blk[item], inst = B.list_inst[item];
+    const long long slot = (long long)tm.x + item;
+    const int blk = from_tape ? __ldg(T.blk + slot) : B.list_blk[item];
+    const int inst = from_tape ? __ldg(T.inst + slot) : B.list_inst[item];
     const InstDev& I = B.inst[inst];
     int i, j, k;
     block_node(I, blk, l, i, j, k);
     const long long n = (long long)blk * 64 + l;
-    const float4 pm = B.grid_pm[n];
+    const float4 pm = from_tape ? __ldg(T.data + slot * 64 + l) : B.grid_pm[n];
     // the rounded reciprocal: measured faster here than the approximate one
     // that the build selects for divisions (16.5 against 20.2 ms per sweep step)
     const float inv_m = __frcp_rn(pm.w + 1e-9f);
@@ -433,12 +457,12 @@ __global__ void __launch_bounds__(256) k_grid(BatchDev B, const float* __restric
       out[0] = __ldg(traj + o); out[1] = __ldg(traj + o + 1); out[2] = __ldg(traj + o + 2);
     }
     B.grid_v[n] = make_float4(out[0], out[1], out[2], 0.f);
-    if (tape_at >= 0) {
-      const long long slot = (long long)tape_at + item;
-      T.data[slot * 64 + l] = pm;
+    if (record_at >= 0) {
+      const long long rs = (long long)record_at + item;
+      T.data[rs * 64 + l] = pm;
       if (l == 0) {
-        T.blk[slot] = blk;
-        T.inst[slot] = inst;
+        T.blk[rs] = blk;
+        T.inst[rs] = inst;
       }
     }
     if (mode == GRID_FORWARD) {
@@ -506,9 +530,9 @@ __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict
   const RestP R = rest_ptrs(rest, B.nv, B.nt, B.no);
   const float dt = B.dt, inv_dx = I.inv_dx;
   if (TRI) {
-    const long long t = ch.start + threadIdx.x, nt = B.nt;
+    const long long t = ch.start + threadIdx.x, nt = B.nt, nv = B.nv;
     TriGeom g;
-    load_tri(B, Si, R, t, false, g);
+    load_centroid(B, Si, t, false, g);
     Sten st;
     make_stencil(g.xc, I, st, B.status, ch.inst);
     float Ct[9];
@@ -527,7 +551,7 @@ __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict
     float dl3[3], d3[3];
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
-      dl3[q] = __ldg(Si.t + (9 + q) * nt + t);
+      dl3[q] = __ldg(Si.t + (TRI_D3 + q) * nt + t);
       d3[q] = __ldg(R.n0 + q * nt + t) + dl3[q];
     }
     // d3 += (dt C + dt^2/2 C C) d3 (simulation.py:397-400), kept as delta3 = d3 - n0
@@ -545,9 +569,26 @@ __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict
       Md[a] = acc;
     }
 #pragma unroll
-    for (int q = 0; q < 9; ++q) So.t[q * nt + t] = Cn[q];
+    for (int q = 0; q < 9; ++q) So.t[(TRI_C + q) * nt + t] = Cn[q];
 #pragma unroll
-    for (int q = 0; q < 3; ++q) So.t[(9 + q) * nt + t] = dl3[q] + Md[q];
+    for (int q = 0; q < 3; ++q) So.t[(TRI_D3 + q) * nt + t] = dl3[q] + Md[q];
+    // centroid and its velocity in the next state (simulation.py:390-393),
+    // from the vertices' new displacements and velocities, which the point
+    // launch of this substep wrote before this launch
+    int vid[3];
+    load_tri_ids(B, t, vid);
+    float su[3], sv[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      su[a] = (So.v[a * nv + vid[0]] + So.v[a * nv + vid[1]]) + So.v[a * nv + vid[2]];
+      sv[a] = (So.v[(3 + a) * nv + vid[0]] + So.v[(3 + a) * nv + vid[1]]) + So.v[(3 + a) * nv + vid[2]];
+    }
+    const float third = 1.f / 3.f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      So.t[(TRI_XC + a) * nt + t] = __ldg(R.tc + a * nt + t) + third * su[a];
+      So.t[(TRI_VC + a) * nt + t] = third * sv[a];
+    }
     return;
   }
   float *ai, *ao;
@@ -612,20 +653,19 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
     if (tri) {
       const long long nt = B.nt;
       if (snext) {
-        const float* cn = snext + 15LL * B.nv;
+        const float* cn = snext + (long long)kPointState * B.nv;
 #pragma unroll
         for (int q = 0; q < 9; ++q) Cn[q] = __ldg(cn + q * nt + idx);
       }
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
-        d3[q] = __ldg(R.n0 + q * nt + idx) + __ldg(Si.t + (9 + q) * nt + idx);
-        bd3o[q] = __ldg(Ao.t + (9 + q) * nt + idx);
+        d3[q] = __ldg(R.n0 + q * nt + idx) + __ldg(Si.t + (TRI_D3 + q) * nt + idx);
+        bd3o[q] = __ldg(Ao.t + (TRI_D3 + q) * nt + idx);
       }
 #pragma unroll
       for (int q = 0; q < 9; ++q) bCo[q] = __ldg(Ao.t + q * nt + idx);
-      TriGeom g;
-      load_tri(B, Si, R, idx, false, g);
-      X[0] = g.xc[0]; X[1] = g.xc[1]; X[2] = g.xc[2];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) X[a] = __ldg(Si.t + (TRI_XC + a) * nt + idx);
     } else {
       point_arrays(B, Si, ch.kind, ai, n);
       point_arrays(B, Ao, ch.kind, ao, n);
@@ -677,7 +717,7 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
         float acc = bd3o[b];
 #pragma unroll
         for (int a = 0; a < 3; ++a) acc += Mm[3 * a + b] * bd3o[a];
-        Ai.t[(9 + b) * nt + idx] = acc;  // partial; k_tri_adj adds the P2G part
+        Ai.t[(TRI_D3 + b) * nt + idx] = acc;  // partial; k_tri_adj adds the P2G part
       }
       // dL/dC' = bCo + dt G + dt^2/2 (G C'^T + C'^T G), G = bd3' d3^T
       float G[9];
@@ -805,19 +845,26 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
   }
 }
 
-// Reverse of k_grid: dL/dp, dL/dm of every active node from dL/dv_out.
+// Reverse of k_grid: dL/dp, dL/dm of every active node from dL/dv_out.  The
+// active blocks and their (p, m) come from the tape when it holds this
+// substep (as in k_grid), otherwise from this substep's recomputed P2G, whose
+// grid and block flags are cleared here for the next substep.
 __global__ void __launch_bounds__(256) k_grid_adj(BatchDev B, const float* __restrict__ params,
                                                   const float* __restrict__ traj, int step, double* __restrict__ gparams,
-                                                  double* __restrict__ gtraj) {
-  const int count = B.counters[0];
+                                                  double* __restrict__ gtraj, TapeP T) {
+  const int2 tm = T.meta ? T.meta[step] : make_int2(-1, 0);
+  const bool from_tape = tm.x >= 0;
+  const int count = from_tape ? tm.y : B.counters[0];
   const int per = blockDim.x >> 6, l = threadIdx.x & 63;
   for (int item = blockIdx.x * per + (threadIdx.x >> 6); item < count; item += gridDim.x * per) {
-    const int blk = B.list_blk[item], inst = B.list_inst[item];
+    const long long slot = (long long)tm.x + item;
+    const int blk = from_tape ? __ldg(T.blk + slot) : B.list_blk[item];
+    const int inst = from_tape ? __ldg(T.inst + slot) : B.list_inst[item];
     const InstDev& I = B.inst[inst];
     int i, j, k;
     block_node(I, blk, l, i, j, k);
     const long long n = (long long)blk * 64 + l;
-    const float4 pm = B.grid_pm[n];
+    const float4 pm = from_tape ? __ldg(T.data + slot * 64 + l) : B.grid_pm[n];
     const float4 ga = B.grid_adj[n];
     const float inv_m = 1.f / (pm.w + 1e-9f);
     const float v[3] = {inv_m * pm.x, inv_m * pm.y, inv_m * pm.z};
@@ -839,8 +886,10 @@ __global__ void __launch_bounds__(256) k_grid_adj(BatchDev B, const float* __res
     const float bp[3] = {inv_m * bv[0], inv_m * bv[1], inv_m * bv[2]};
     const float bm = -inv_m * (bv[0] * v[0] + bv[1] * v[1] + bv[2] * v[2]);
     B.grid_adj[n] = make_float4(bp[0], bp[1], bp[2], bm);
-    B.grid_pm[n] = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (l == 0) B.flags[blk] = 0u;
+    if (!from_tape) {
+      B.grid_pm[n] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (l == 0) B.flags[blk] = 0u;
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) gmu += __shfl_xor_sync(0xffffffffu, gmu, o);
     if ((threadIdx.x & 31) == 0 && gmu != 0.f) atomicAdd(gparams + inst * PRM_STRIDE + PRM_FRICTION, (double)gmu);
@@ -1000,16 +1049,18 @@ __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* 
   const float ks = prm[PRM_KS], kc = prm[PRM_KC];
   float gsum[4] = {0.f, 0.f, 0.f, 0.f};
   if (valid) {
-    float C[9], dl3[3], n0[3], Di[9];   // own loads first, overlapping the vertex gathers
+    float C[9], dl3[3], n0[3], Di[9], e[6];   // own loads first, overlapping the vertex gathers
 #pragma unroll
     for (int q = 0; q < 9; ++q) C[q] = __ldg(Si.t + q * nt + t);
     load_tri_rest(B, R, Si, t, dl3, n0, Di);
+    load_rest_edges(B, R, t, e);
     TriGeom g;
-    load_tri(B, Si, R, t, true, g);
+    load_centroid(B, Si, t, true, g);
+    load_corner_u(B, Si, t, g);
     Sten st;
     make_stencil(g.xc, I, st, B.status, ch.inst);
     M3<float> d, Fe;
-    tri_F(g, dl3, n0, Di, d, Fe);
+    tri_F(g, e, dl3, n0, Di, d, Fe);
     const float d3[3] = {d.m[2], d.m[5], d.m[8]};
     // The stencil loop needs only P's third column, which depends on the QR
     // alone: P[:,2] = Q (A R^-T)[:,2] = k_s (r02 q1 + r12 q2) + A22 / n3 q3
@@ -1171,7 +1222,7 @@ __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* 
 #pragma unroll
     for (int q = 0; q < 9; ++q) Ai.t[q * nt + t] = m * spd[q];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) Ai.t[(9 + a) * nt + t] += bd3[a];
+    for (int a = 0; a < 3; ++a) Ai.t[(TRI_D3 + a) * nt + t] += bd3[a];
     // (mu, la) -> (E, nu)
     const float dmu_dE = 1.f / (2.f * (1.f + nu)), dmu_dnu = -E / (2.f * (1.f + nu) * (1.f + nu));
     const float D = (1.f + nu) * (1.f - 2.f * nu);
@@ -1316,26 +1367,35 @@ __global__ void __launch_bounds__(256) k_reset_tri(BatchDev B, float* __restrict
                                                    float* __restrict__ fdev) {
   StateP S = state_ptrs(state, B.nv, B.nt, B.no);
   const RestP R = rest_ptrs(rest, B.nv, B.nt, B.no);
-  const long long nt = B.nt;
+  const long long nt = B.nt, nv = B.nv;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nt; t += (long long)gridDim.x * blockDim.x) {
     TriGeom g;
-    load_tri(B, S, R, t, false, g);
-    float dl3[3], n0[3], Di[9];
+    load_corner_u(B, S, t, g);
+    float dl3[3], n0[3], Di[9], e[6];
     load_tri_rest(B, R, S, t, dl3, n0, Di);
+    load_rest_edges(B, R, t, e);
     M3<float> d, Fe;
-    tri_F(g, dl3, n0, Di, d, Fe);
+    tri_F(g, e, dl3, n0, Di, d, Fe);
     for (int q = 0; q < 9; ++q) fdev[q * nt + t] = Fe.m[q];
     float p[3][3];
     for (int c = 0; c < 3; ++c)
-      for (int a = 0; a < 3; ++a) p[c][a] = g.X0[c][a] + g.U[c][a];
+      for (int a = 0; a < 3; ++a) p[c][a] = R.xv[a * nv + g.vid[c]] + g.U[c][a];
     float inv[9], nrm[3];
     rest_frame(p[0], p[1], p[2], inv, nrm);
     float* DiW = const_cast<float*>(R.Di);
     float* n0W = const_cast<float*>(R.n0);
+    float* eW = const_cast<float*>(R.e);
+    float* tcW = const_cast<float*>(R.tc);
     for (int q = 0; q < 9; ++q) DiW[q * nt + t] = inv[q];
     for (int q = 0; q < 3; ++q) {
       n0W[q * nt + t] = nrm[q];
-      S.t[(9 + q) * nt + t] = 0.f;
+      eW[q * nt + t] = p[1][q] - p[0][q];
+      eW[(3 + q) * nt + t] = p[2][q] - p[0][q];
+      // the kept centroid becomes the rest centroid: the vertices' rest
+      // positions move to their current ones (k_reset_vertex) and their
+      // displacements become 0
+      tcW[q * nt + t] = S.t[(TRI_XC + q) * nt + t];
+      S.t[(TRI_D3 + q) * nt + t] = 0.f;
     }
   }
 }
@@ -1368,26 +1428,6 @@ __global__ void k_tape_reserve(BatchDev B, TapeP T, int step) {
   }
 }
 
-// Restore the (p, m) grid and the active-block list of substep `step`.
-__global__ void __launch_bounds__(256) k_tape_restore(BatchDev B, TapeP T, int step) {
-  const int2 m = T.meta[step];
-  if (m.x < 0) return;
-  if (blockIdx.x == 0 && threadIdx.x == 0) B.counters[0] = m.y;
-  const long long total = (long long)m.y * 64;
-  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
-    const long long item = g >> 6;
-    const int l = (int)(g & 63);
-    const long long slot = m.x + item;
-    const int blk = __ldg(T.blk + slot);
-    B.grid_pm[(long long)blk * 64 + l] = __ldg(T.data + slot * 64 + l);
-    if (l == 0) {
-      B.list_blk[item] = blk;
-      B.list_inst[item] = __ldg(T.inst + slot);
-      B.flags[blk] = 1u;
-    }
-  }
-}
-
 // ============================================================== launchers
 const char* const kKernelNames[KID_COUNT] = {
     "k_tri_forward", "k_point_p2g", "k_grid", "k_g2p", "k_g2p_adj", "k_grid_adj", "k_point_adj", "k_tri_adj",
@@ -1407,7 +1447,7 @@ static inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) 
 cudaError_t launch_init(const BatchDev& B, const LaunchCfg& L, const float* x0v, const float* x0o, const float* x0c,
                         float* state, float* rest, cudaStream_t s) {
   const long long total = (long long)B.nv + B.no + B.nc + B.nt;
-  const int grid = total > 0 ? (ceil_div(total, 256) < 148 * 16 ? ceil_div(total, 256) : 148 * 16) : 1;
+  const int grid = total > 0 ? std::min(ceil_div(total, 256), L.sm_count * 16) : 1;
   DCP_LAUNCH(KID_INIT, (k_init<<<grid, 256, 0, s>>>(B, x0v, x0o, x0c, state, rest)));
   return cudaGetLastError();
 }
@@ -1417,11 +1457,11 @@ cudaError_t launch_init(const BatchDev& B, const LaunchCfg& L, const float* x0v,
 cudaError_t launch_reset(const BatchDev& B, const LaunchCfg& L, float* rest, float* state, float* fdev,
                          cudaStream_t s) {
   if (B.nt) {
-    const int grid = std::min(ceil_div(B.nt, 256), 148 * 16);
+    const int grid = std::min(ceil_div(B.nt, 256), L.sm_count * 16);
     DCP_LAUNCH(KID_RESET, (k_reset_tri<<<grid, 256, 0, s>>>(B, rest, state, fdev)));
   }
   if (B.nv) {
-    const int grid = std::min(ceil_div(B.nv, 256), 148 * 16);
+    const int grid = std::min(ceil_div(B.nv, 256), L.sm_count * 16);
     DCP_LAUNCH(KID_RESET, (k_reset_vertex<<<grid, 256, 0, s>>>(B, rest, state)));
   }
   return cudaGetLastError();
@@ -1447,10 +1487,11 @@ cudaError_t launch_forward(const BatchDev& B, const LaunchCfg& L, const float* p
                                   T ? tp.fv + (long long)step * 3 * B.nv : nullptr, 1)));
   if (T) DCP_LAUNCH(KID_TAPE, (k_tape_reserve<<<1, 32, 0, s>>>(B, tp, step)));
   DCP_LAUNCH(KID_GRID, (k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_FORWARD, tp)));
-  if (B.n_tri_chunks)
-    DCP_LAUNCH(KID_G2P, (k_g2p<true><<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin, sout)));
+  // points first: the triangle launch forms the next centroids from the vertices' new state
   if (B.n_point_chunks)
     DCP_LAUNCH(KID_G2P, (k_g2p<false><<<B.n_point_chunks, L.block, 0, s>>>(B, params, rest, sin, sout)));
+  if (B.n_tri_chunks)
+    DCP_LAUNCH(KID_G2P, (k_g2p<true><<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin, sout)));
   return cudaGetLastError();
 }
 
@@ -1458,10 +1499,9 @@ cudaError_t launch_backward(const BatchDev& B, const LaunchCfg& L, const float* 
                             const float* rest, int step, int window, const float* sin, const float* aout, float* ain,
                             double* gparams, double* gtraj, cudaStream_t s, const TapeP* T, const float* snext,
                             bool fold, bool collect) {
-  const TapeP none = no_tape();
+  const TapeP tp = T ? *T : no_tape();
   const int2* meta = T ? T->meta + step : nullptr;
   cudaMemsetAsync(B.counters, 0, sizeof(int), s);
-  if (T) DCP_LAUNCH(KID_TAPE, (k_tape_restore<<<L.grid_ctas, 256, 0, s>>>(B, *T, step)));
   // with a tape the P2G recompute usually returns at once: launch a few CTAs
   // per SM that stride over the chunks instead of one CTA per chunk
   const int stride_ctas = 2 * L.grid_ctas;
@@ -1473,10 +1513,10 @@ cudaError_t launch_backward(const BatchDev& B, const LaunchCfg& L, const float* 
   if (B.n_point_chunks)
     DCP_LAUNCH(KID_POINT_P2G, (k_point_p2g<<<point_ctas, L.block, 0, s>>>(B, traj, step, window, rest, sin,
                                                                          meta, nullptr, 0)));
-  DCP_LAUNCH(KID_GRID, (k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_RECOMPUTE, none)));
+  DCP_LAUNCH(KID_GRID, (k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_RECOMPUTE, tp)));
   DCP_LAUNCH(KID_G2P_ADJ, (DCP_MINB(k_g2p_adj, L, 1)<<<B.n_tri_chunks + B.n_point_chunks, L.block, 0, s>>>(
                               B, params, rest, sin, aout, ain, gparams, snext, fold ? 1 : 0)));
-  DCP_LAUNCH(KID_GRID_ADJ, (k_grid_adj<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, gparams, gtraj)));
+  DCP_LAUNCH(KID_GRID_ADJ, (k_grid_adj<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, gparams, gtraj, tp)));
   if (B.n_point_chunks)
     DCP_LAUNCH(KID_POINT_ADJ, (k_point_adj<<<B.n_point_chunks, L.block, 0, s>>>(
                                   B, traj, step, window, rest, sin, ain, gtraj, meta,

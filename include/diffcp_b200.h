@@ -23,13 +23,19 @@
  * State snapshot (floats, dcp_plan().state_floats), relative to the rest
  * configuration so that float32 resolves small strains:
  *   [15][Nv] vertices  u(3) v(3) C(9, row-major)   u = x - x0
- *   [12][Nt] triangles C(9) delta3(3)   delta3 = d3 - n0, d3 the advected third
- *                                       column of d (columns 1-2 of d are the
- *                                       current edges)
+ *   [18][Nt] triangles C(9) delta3(3) xc(3) vc(3)
+ *                      delta3 = d3 - n0, d3 the advected third column of d
+ *                      (columns 1-2 of d are the current edges); xc, vc the
+ *                      centroid's absolute position and velocity (the
+ *                      reference's quadrature_x / quadrature_v, simulation.py:
+ *                      390-393), written with every state from its vertices
+ *                      (a caller that edits a state's vertex displacements or
+ *                      velocities directly must update these to match)
  *   [15][No] operator particles u v C
  *   [15][Nc] cube particles     u v C
  * Rest buffer (floats, dcp_plan().rest_floats), written by dcp_init_state:
- *   [9][Nt] D0^-1, [3][Nt] n0, [3][Nv] x0, [3][No] x0, [3][Nc] x0
+ *   [9][Nt] D0^-1, [3][Nt] n0, [6][Nt] rest edges (D0's first two columns),
+ *   [3][Nt] rest centroids, [3][Nv] x0, [3][No] x0, [3][Nc] x0
  * Parameter table: [n_inst][8] floats: E, nu, shearing_stiffness,
  *   contact_stiffness, ground friction, damping, 0, 0.
  * Parameter gradients: [n_inst][8] doubles in the same order (accumulated).

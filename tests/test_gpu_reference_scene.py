@@ -1,6 +1,6 @@
 """The drop-in module (diffcp_b200.reference_api) on the reference's own scene
-(data/cloth_mesh.ply, the first grasp frames and target windows; 30 substeps
-per window), driven through compute_grad() itself, so that each window starts
+(data/cloth_mesh.ply, the first grasp frames and target windows; 300
+substeps per window), driven through compute_grad() itself, so that each window starts
 from the previous window's end state (parameter_fitting_functions.py:40-49).
 Compared with the reference source run on the same tree
 (tests/golden/ref_real_f32.npz, ref_real_fd_f64.npz): every window's loss and
@@ -17,7 +17,7 @@ from tests.ref_tree import write_real_tree
 
 pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
-MIN_SENSITIVITY = 1e-5   # see tests/test_oracle_real_scene.py
+MIN_SENSITIVITY = 5e-6   # see tests/test_oracle_real_scene.py
 
 
 @pytest.fixture(scope="module")
@@ -56,7 +56,7 @@ def run(tmp_path_factory):
 
 def test_every_window_matches_reference_source(run):
     gold, fd, windows, loss_mean = run
-    assert len(windows) == int(gold["n_windows"]) == 3
+    assert len(windows) == int(gold["n_windows"]) == 2
     for g, w in enumerate(windows):
         ref_hist = gold["w%d_vertex_x" % g]
         assert w["vx"].shape == ref_hist.shape

@@ -59,7 +59,7 @@ def test_plan_sizes_and_validation():
     s = native.DcpSizes()
     assert L.dcp_plan(insts, 2, ctypes.byref(opt), ctypes.byref(s)) == 0
     assert s.n_vertex == 32 and s.n_tri == 36 and s.n_target == 7
-    assert s.state_floats == 15 * 32 + 12 * 36
+    assert s.state_floats == 15 * 32 + 18 * 36
     assert s.total_nodes == 4 ** 3 * 64 * 2      # 15 nodes per axis pad to 4 blocks of 4
     assert s.n_tri_chunks == 2 and s.n_point_chunks == 2
     bad = native.DcpOptions(dt=1e-4, chunk=100, svd_grad=0, grid_ctas=0)

@@ -1,12 +1,12 @@
 """The reference's own scene (data/cloth_mesh.ply: 427 vertices, 777
 triangles, binary float64; the first grasp frames of grasp_traj_array.npy; the
-first target windows of target_pcd_sample.npy) with a short horizon of 30
+first target windows of target_pcd_sample.npy) with a short horizon of 300
 substeps per window, against golden vectors of the reference source run on it
 (tests/golden/make_golden.py, modes real32 and real64):
 
   * the product's PLY reader on the reference's binary file;
   * the product's scene loader: the constants of src/initialization.py;
-  * the FP64 oracle over three grasp windows with the end-state carry-over of
+  * the FP64 oracle over two grasp windows with the end-state carry-over of
     compute_grad (parameter_fitting_functions.py:40-49): vertex histories and
     per-window losses;
   * the oracle's window-1 gradients against central differences of the
@@ -29,8 +29,11 @@ from tests.ref_tree import write_real_tree
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 # relative sensitivity |dL/dp| p / L below which a float64 central difference
-# with h = 1e-4 p cannot pin a gradient to 2e-4
-MIN_SENSITIVITY = 1e-5
+# with h = 1e-4 p cannot pin a gradient to 2e-4 (the float64 loss carries
+# rounding of about 1e-13 of itself, so the quotient errs by ~1e-9 / sensitivity;
+# over one 300-substep window of the reference's soft cloth, E = 100 Pa, the
+# Poisson ratio and the contact stiffness stay below it)
+MIN_SENSITIVITY = 5e-6
 
 
 def _load(name):
@@ -123,7 +126,7 @@ def test_product_scene_loader_matches_reference_constants(gold, tree):
 def test_oracle_windows_with_carry_over_match_reference_source(gold, tree):
     sc = oracle_scene(tree)
     n_win = int(gold["n_windows"])
-    assert n_win == 3 and sc["max_steps"] == 31
+    assert n_win == 2 and sc["max_steps"] == 301
     params = _params(gold["params"])
     seq = torch.tensor(sc["grasp_point_pos"], dtype=torch.float64)
     init = (sc["vertices"], sc["operator_x"], sc["cube_x"])
