@@ -402,6 +402,14 @@ def main():
     step()
     torch.cuda.synchronize()
     prof = batch.profile_read()
+    # particle order kept from the start of the rollout: do the forward
+    # scatters slow down as the cloth moves away from its initial Morton order?
+    order_drift = {}
+    for name in ("k_tri_forward", "k_point_p2g"):
+        t = batch.profile_launches(name)[: info["n_steps"]]    # the forward rollout, substeps 0 .. n-1
+        if len(t) >= 60:
+            order_drift[name] = {"first30_ms": float(np.mean(t[:30])), "last30_ms": float(np.mean(t[-30:])),
+                                 "last_over_first": float(np.mean(t[-30:]) / np.mean(t[:30]))}
     batch.profile(False)
     sim.use_graph = True
     n_nodes_active = None
@@ -465,6 +473,7 @@ def main():
                           "frac": step_alg / (ms_max / 1e3) / 1e9 / peak,
                           "bytes_per_particle": STEP_BYTES},
         "kernels": kernels,
+        "order_drift": order_drift,
         "cpu_baseline": cpu,
         "single_instance": single,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

@@ -314,6 +314,17 @@ class ClothBatch:
         check(self.lib.dcp_profile_read(self.handle, ms, n), "dcp_profile_read")
         return {self.lib.dcp_kernel_name(i).decode(): (ms[i], n[i]) for i in range(k) if n[i]}
 
+    def profile_launches(self, name: str) -> np.ndarray:
+        """Milliseconds of every profiled launch of kernel ``name``, in launch order."""
+        names = [self.lib.dcp_kernel_name(i).decode() for i in range(int(self.lib.dcp_kernel_count()))]
+        kid = names.index(name)
+        n = int(self.lib.dcp_profile_launches(self.handle, kid, None, 0))
+        out = (ctypes.c_double * max(n, 1))()
+        got = int(self.lib.dcp_profile_launches(self.handle, kid, out, n))
+        if got < 0:
+            check(1, "dcp_profile_launches")
+        return np.array(out[:n])
+
     def status(self, clear: bool = True) -> np.ndarray:
         out = (ctypes.c_int32 * self.n_inst)()
         check(self.lib.dcp_read_status(self.handle, out, int(clear), _stream()), "dcp_read_status")

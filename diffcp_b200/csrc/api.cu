@@ -614,6 +614,29 @@ int dcp_profile_read(DcpBatch* b, double* total_ms, int64_t* launches) {
   return DCP_OK;
 }
 
+int64_t dcp_profile_launches(DcpBatch* b, int32_t id, double* ms, int64_t cap) {
+  if (!b || id < 0 || id >= KID_COUNT || (cap > 0 && !ms)) {
+    fail(DCP_ERR_INVALID, "dcp_profile_launches: bad argument");
+    return -1;
+  }
+  int64_t n = 0;
+  for (auto& r : b->prof.recs) {
+    if (r.id != id) continue;
+    if (n < cap) {
+      cudaError_t e = cudaEventSynchronize(r.b);
+      float t = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&t, r.a, r.b);
+      if (e != cudaSuccess) {
+        cuda_fail(e, "dcp_profile_launches");
+        return -1;
+      }
+      ms[n] = t;
+    }
+    ++n;
+  }
+  return n;
+}
+
 int dcp_read_status(DcpBatch* b, int32_t* host_status, int32_t clear, void* stream) {
   if (!b || !host_status) return fail(DCP_ERR_INVALID, "NULL argument");
   cudaStream_t s = (cudaStream_t)stream;

@@ -362,14 +362,17 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
       }
 }
 
-// Warp + CTA sum of up to 8 doubles, one atomic per value per CTA.
+// Warp + CTA sum of up to 8 per-thread parameter-gradient contributions, in
+// double from the thread on (contributions of both signs cancel over a
+// rollout, so float partial sums would set the gradient's error), one atomic
+// per value per CTA.
 template <int N>
-__device__ __forceinline__ void block_sum_atomic(float (&vals)[N], double* dst) {
-  __shared__ float red[N][32];
+__device__ __forceinline__ void block_sum_atomic(double (&vals)[N], double* dst) {
+  __shared__ double red[N][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
 #pragma unroll
   for (int a = 0; a < N; ++a) {
-    float v = vals[a];
+    double v = vals[a];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (lane == 0) red[a][warp] = v;
@@ -377,7 +380,7 @@ __device__ __forceinline__ void block_sum_atomic(float (&vals)[N], double* dst) 
   __syncthreads();
   if (threadIdx.x < N) {
     double s = 0.0;
-    for (int w = 0; w < nw; ++w) s += (double)red[threadIdx.x][w];
+    for (int w = 0; w < nw; ++w) s += red[threadIdx.x][w];
     if (s != 0.0) atomicAdd(dst + threadIdx.x, s);
   }
   __syncthreads();

@@ -641,7 +641,7 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
   const bool tri = ch.kind == CHUNK_TRI;
   const long long idx = ch.start + tid;
   Sten st;
-  float gdamp[1] = {0.f};
+  double gdamp[1] = {0.0};
   float bV[3] = {0.f, 0.f, 0.f}, Kg[3] = {0.f, 0.f, 0.f};  // dL/dv', node weight base
   float cbC[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // 4/dx dL/dC of the gather
   if (valid) {
@@ -741,7 +741,7 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
       float gd = 0.f;
 #pragma unroll
       for (int q = 0; q < 9; ++q) gd -= bCn[q] * sym[q];
-      gdamp[0] = gd;
+      gdamp[0] = (double)gd;
 #pragma unroll
       for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -891,8 +891,9 @@ __global__ void __launch_bounds__(256) k_grid_adj(BatchDev B, const float* __res
       if (l == 0) B.flags[blk] = 0u;
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) gmu += __shfl_xor_sync(0xffffffffu, gmu, o);
-    if ((threadIdx.x & 31) == 0 && gmu != 0.f) atomicAdd(gparams + inst * PRM_STRIDE + PRM_FRICTION, (double)gmu);
+    double gmud = (double)gmu;
+    for (int o = 16; o > 0; o >>= 1) gmud += __shfl_xor_sync(0xffffffffu, gmud, o);
+    if ((threadIdx.x & 31) == 0 && gmud != 0.0) atomicAdd(gparams + inst * PRM_STRIDE + PRM_FRICTION, gmud);
   }
 }
 
@@ -1047,7 +1048,7 @@ __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* 
   float mu, la;
   lame(E, nu, mu, la);
   const float ks = prm[PRM_KS], kc = prm[PRM_KC];
-  float gsum[4] = {0.f, 0.f, 0.f, 0.f};
+  double gsum[4] = {0.0, 0.0, 0.0, 0.0};
   if (valid) {
     float C[9], dl3[3], n0[3], Di[9], e[6];   // own loads first, overlapping the vertex gathers
 #pragma unroll
@@ -1227,10 +1228,11 @@ __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* 
     const float dmu_dE = 1.f / (2.f * (1.f + nu)), dmu_dnu = -E / (2.f * (1.f + nu) * (1.f + nu));
     const float D = (1.f + nu) * (1.f - 2.f * nu);
     const float dla_dE = nu / D, dla_dnu = E * (1.f + 2.f * nu * nu) / (D * D);
-    gsum[0] = gmu * dmu_dE + gla * dla_dE;
-    gsum[1] = gmu * dmu_dnu + gla * dla_dnu;
-    gsum[2] = gks;
-    gsum[3] = gkc;
+    // the (mu, lambda) -> (E, nu) chain in double: the two terms cancel in part
+    gsum[0] = (double)gmu * (double)dmu_dE + (double)gla * (double)dla_dE;
+    gsum[1] = (double)gmu * (double)dmu_dnu + (double)gla * (double)dla_dnu;
+    gsum[2] = (double)gks;
+    gsum[3] = (double)gkc;
   }
   block_sum_atomic<4>(gsum, gparams + ch.inst * PRM_STRIDE);
 }

@@ -27,7 +27,7 @@ EXPORTED = (
     "dcp_plan", "dcp_create", "dcp_destroy", "dcp_sizes", "dcp_init_state", "dcp_substep_forward",
     "dcp_substep_backward", "dcp_chamfer_forward", "dcp_chamfer_backward", "dcp_rollout_floats", "dcp_tape_bytes", "dcp_reset_quadrature", "dcp_replay",
     "dcp_rollout_state_offset", "dcp_rollout_forward", "dcp_rollout_backward", "dcp_read_status", "dcp_last_error",
-    "dcp_launch_count", "dcp_profile", "dcp_profile_read", "dcp_kernel_count", "dcp_kernel_name",
+    "dcp_launch_count", "dcp_profile", "dcp_profile_read", "dcp_profile_launches", "dcp_kernel_count", "dcp_kernel_name",
     "dcp_chamfer_forward_static",
 )
 STATIC_MAX_TARGETS = 1 << 20
@@ -109,6 +109,8 @@ def lib():
     L.dcp_launch_count.restype = c_int64
     L.dcp_profile.argtypes = [c_void_p, c_int32]
     L.dcp_profile_read.argtypes = [c_void_p, P(ctypes.c_double), P(c_int64)]
+    L.dcp_profile_launches.argtypes = [c_void_p, c_int32, P(ctypes.c_double), c_int64]
+    L.dcp_profile_launches.restype = c_int64
     L.dcp_kernel_count.restype = c_int32
     L.dcp_kernel_name.argtypes = [c_int32]
     L.dcp_kernel_name.restype = ctypes.c_char_p

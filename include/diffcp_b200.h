@@ -222,6 +222,9 @@ int dcp_rollout_backward(DcpBatch* batch, const float* params, const float* traj
 int64_t dcp_launch_count(const DcpBatch* batch);
 int dcp_profile(DcpBatch* batch, int32_t enable);
 int dcp_profile_read(DcpBatch* batch, double* total_ms, int64_t* launches);
+/* Milliseconds of each profiled launch of kernel `id`, in launch order, into
+ * ms[0 .. cap); returns the number of such launches (-1 on error). */
+int64_t dcp_profile_launches(DcpBatch* batch, int32_t id, double* ms, int64_t cap);
 int32_t dcp_kernel_count(void);
 const char* dcp_kernel_name(int32_t id);
 
