@@ -12,10 +12,12 @@
   trajectory_batch 64 sheets of 64x64 vertices, 96^3 grids, 400 substeps, per-
                    substep gripper velocities N(0, 0.01 m/s); targets from the
                    final state under another velocity draw
-  stress_sheet     a 512x512-vertex sheet, 256^3 grid, dt 5e-5, 2000 substeps,
-                   checkpoints every 45; 0.85 m side instead of 1 m, because
-                   the simulation domain is the unit cube with 3-cell sticky
-                   walls and the grasped corners move by up to 5 cm
+  stress_sheet     a 512x512-vertex sheet of 1 m side, 256^3 grid, dt 5e-5,
+                   2000 substeps, checkpoints every 45; the domain is the unit
+                   cube with 3-cell sticky walls (interior 0.977 m wide), so
+                   the sheet's rest shape is a shallow bowl (radius 0.8 m:
+                   0.936 m wide, edges still 1/511 m) and its grasped corners
+                   move by up to 1 cm instead of 5
 
 Targets that come from a simulated final state are computed with this
 library on the GPU (``final_state_targets``).
@@ -121,7 +123,8 @@ def trajectory_batch(seed: int = 0, count: int = 64, n: int = 64, n_steps: int =
 
 
 def stress_sheet(seed: int = 0) -> Tuple[List[scene.ClothScene], dict]:
-    return [scene.sheet_scene(n=512, side=0.85, height=0.3, n_grid=256, dt=5e-5, n_steps=2000, seed=seed,
-                              n_targets=2048)], dict(
+    return [scene.sheet_scene(n=512, side=1.0, height=0.2, n_grid=256, dt=5e-5, n_steps=2000, seed=seed,
+                              n_targets=2048, cap_radius=0.8, grasp_amplitude=0.01)], dict(
         dt=5e-5, n_steps=2000, ckpt_every=45,
-        desc="stress: one cloth 512x512 vertices, 0.85 m, 256^3 grid, dt 5e-5, 2000 substeps, checkpoints every 45")
+        desc="stress: one cloth 512x512 vertices, 1 m side (bowl-shaped rest, 0.936 m wide), 256^3 grid, dt 5e-5, "
+             "2000 substeps, checkpoints every 45")

@@ -210,17 +210,33 @@ def sheet_scene(n: int = 32, side: float = 0.2, height: float = 0.3, n_grid: int
                 n_steps: int = 200, E: float = 5e3, nu: float = 0.3, density: float = 0.2, friction: float = 0.3,
                 damping: float = REFERENCE_DAMPING, seed: int = 0, n_targets: int = 2048,
                 gripper_radius: Optional[float] = None, center=(0.5, 0.5), velocities=None,
-                spline_duration: float = 1.0) -> ClothScene:
+                spline_duration: float = 1.0, cap_radius: Optional[float] = None,
+                grasp_amplitude: float = 0.05) -> ClothScene:
     """Square cloth sheet held by two kinematic spheres at two adjacent
     corners, the cloth of the benchmark configurations.  Masses follow the
     reference's formulas (initialization.py:118-130) with the garment mass set
     from the areal ``density``; gravity is not scaled (scene_scaling = 1).
     ``velocities`` (n_steps, 2, 3) replaces the spline with per-substep
-    gripper velocities (centres integrate them)."""
+    gripper velocities (centres integrate them).
+
+    ``cap_radius`` R: the sheet's rest shape is a shallow bowl instead of a
+    plane: the point at in-plane offsets (u, v) from the centre sits at
+    (R sin(u/R), R (2 - cos(u/R) - cos(v/R)), R sin(v/R)) relative to the
+    centre at ``height``, so the mesh keeps its side length along both mesh
+    directions (edges of side / (n - 1)) while its horizontal extent shrinks
+    to 2 R sin(side / 2R).  A sheet as wide as the domain fits between the
+    walls this way."""
     rng = np.random.default_rng(seed)
     verts, tris = regular_sheet(n, side)
-    verts = verts + np.array([center[0] - side / 2, height, center[1] - side / 2])
-    area = side * side
+    if cap_radius is None:
+        verts = verts + np.array([center[0] - side / 2, height, center[1] - side / 2])
+        area = side * side
+    else:
+        R = float(cap_radius)
+        u, v = verts[:, 0] - side / 2, verts[:, 2] - side / 2
+        verts = np.stack([center[0] + R * np.sin(u / R), height + R * (2.0 - np.cos(u / R) - np.cos(v / R)),
+                          center[1] + R * np.sin(v / R)], -1)
+        area = mesh_area(verts, tris)
     dx = 1.0 / n_grid
     M = density * area
     corners = np.stack([verts[0], verts[n - 1]])   # (0,0) and (0,n-1): adjacent corners
@@ -228,7 +244,8 @@ def sheet_scene(n: int = 32, side: float = 0.2, height: float = 0.3, n_grid: int
         vel = np.zeros((n_steps, 2, 3))
         cen = np.zeros((n_steps, 2, 3))
         for k in range(2):
-            vel[:, k], cen[:, k] = cubic_spline_grasp(corners[k], n_steps, dt, rng, duration=spline_duration)
+            vel[:, k], cen[:, k] = cubic_spline_grasp(corners[k], n_steps, dt, rng, amplitude=grasp_amplitude,
+                                                      duration=spline_duration)
     else:
         vel = np.asarray(velocities, dtype=np.float64).reshape(n_steps, 2, 3)
         cen = corners[None] + dt * np.concatenate([np.zeros((1, 2, 3)), np.cumsum(vel, 0)[:-1]], 0)
