@@ -158,59 +158,47 @@ def median_instance(scenes):
     return i, scenes[i]
 
 
+def cpu_sample(scenes, k):
+    """k instances spread evenly over the workload's sizes (sorted by particle
+    count), so that the sample has the workload's mix of cloth sizes."""
+    order = np.argsort([s.n_vertex + s.n_tri for s in scenes], kind="stable")
+    idx = sorted({int(order[int(round(j * (len(scenes) - 1) / max(k - 1, 1)))]) for j in range(k)})
+    return idx
+
+
 def cpu_rate(scenes, info, seconds=15.0, steps=1, warmup=0, min_substeps=20):
-    """Oracle (torch, float32, all host threads) fwd+bwd rate on a bounded
-    sample of the workload: the instance nearest the median size.  Each of
-    ``steps`` timed steps is the forward and adjoint of ``n`` substeps of it,
-    n >= ``min_substeps`` sized so that the timed steps take about
-    ``seconds``; the oracle's set-up (rest frames, state 0) is outside the
-    timed region, as the GPU arm's is."""
-    import torch
-    from oracle import sim64
-    from oracle.sim64 import Constants, KinematicGripper, OracleSim
-    idx, sc = median_instance(scenes)
-    dt = info["dt"]
-    d = torch.float32
-    const = Constants(n_grid=sc.n_grid, dt=dt, vertex_p_mass=sc.vertex_p_mass, quadrature_p_mass=sc.quadrature_p_mass,
-                      quadrature_p_vol=sc.quadrature_p_vol, gravity_dv=sc.gravity_dv, bound=sc.bound)
-    targets = torch.tensor(sc.targets, dtype=d)
-
-    def setup():
-        osim, st = OracleSim.initialize(const, sc.vertices, sc.triangles, dtype=d)
-        p = {k: torch.tensor(float(v), dtype=d, requires_grad=True) for k, v in
-             zip(("E", "nu", "ks", "kc", "friction", "damping"), sc.param_row())}
-        vel = torch.tensor(sc.velocities, dtype=d, requires_grad=True)
-        grip = KinematicGripper(sc.gripper_radius, torch.tensor(sc.centers, dtype=d), vel)
-        return osim, st, p, grip
-
-    def run(n, ready):
-        osim, st, p, grip = ready
-        for f in range(n):
-            st = osim.substep(st, f, 0, p, friction=p["friction"], damping=p["damping"], grip=grip)
-        lo, _ = sim64.compute_loss(st["vx"], targets)
-        lo.backward()
-
-    ready = setup()
+    """The CPU baseline: oracle/cpu_port.cpp, the compiled float32 restatement
+    of the substep and its adjoint (the reference's Taichi is not installed),
+    on all host cores, one OpenMP thread per cloth.  A bounded sample of the
+    workload: as many cloths as threads, spread over its sizes, each timed
+    step the forward rollout, Chamfer loss and reverse pass of n >=
+    ``min_substeps`` substeps of each, n sized so that the timed steps take
+    about ``seconds``."""
+    from oracle import cpu_port
+    threads = os.cpu_count() or 1
+    idx = cpu_sample(scenes, min(threads, len(scenes)))
+    sample = [scenes[i] for i in idx]
+    parts = sum(s.n_vertex + s.n_tri for s in sample)
+    cpu_port.rollouts(sample, 2, threads)              # set-up, first touch, thread pool
     t0 = time.perf_counter()
-    run(2, ready)
+    cpu_port.rollouts(sample, 2, threads)
     per = (time.perf_counter() - t0) / 2
-    n = int(max(min_substeps, min(info["n_steps"], seconds / max(steps, 1) / max(per, 1e-3))))
+    n = int(max(min_substeps, min(info["n_steps"], seconds / max(steps, 1) / max(per, 1e-4))))
     for _ in range(warmup):
-        run(2, setup())
+        cpu_port.rollouts(sample, 2, threads)
     el = 0.0
     k = max(steps, 1)
     for _ in range(k):
-        ready = setup()
         t0 = time.perf_counter()
-        run(n, ready)
+        cpu_port.rollouts(sample, n, threads)
         el += time.perf_counter() - t0
-    rate = (sc.n_vertex + sc.n_tri) * n * k / el
-    return {"value": rate, "unit": UNIT, "cores": torch.get_num_threads(), "kind": "port",
-            "ms_per_step": 1e3 * el / k, "instance": idx, "substeps_per_step": n,
-            "sample": "CPU oracle port (torch float32, %d threads; the reference's Taichi is not installed) fwd+bwd "
-                      "of %d substeps of instance %d of the workload (%d vertices + %d triangles, the median size) "
-                      "per step, %d timed step(s) in %.1f s, set-up outside the timed region" % (
-                          torch.get_num_threads(), n, idx, sc.n_vertex, sc.n_tri, k, el)}
+    rate = parts * n * k / el
+    return {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "ms_per_step": 1e3 * el / k,
+            "instances": idx, "substeps_per_step": n,
+            "sample": "compiled float32 CPU restatement of the substep and its adjoint (oracle/cpu_port.cpp; the "
+                      "reference's Taichi is not installed), %d threads, one cloth each: %d cloths of the workload "
+                      "spread over its sizes (%d particles), fwd+bwd of %d substeps per step, %d timed step(s) in "
+                      "%.1f s" % (threads, len(sample), parts, n, k, el)}
 
 
 def workload_config(scenes, info, world=1):

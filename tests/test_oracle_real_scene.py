@@ -6,12 +6,11 @@ substeps per window, against golden vectors of the reference source run on it
 
   * the product's PLY reader on the reference's binary file;
   * the product's scene loader: the constants of src/initialization.py;
-  * the FP64 oracle over two grasp windows with the end-state carry-over of
-    compute_grad (parameter_fitting_functions.py:40-49): vertex histories and
-    per-window losses;
-  * the oracle's window-1 gradients against central differences of the
-    reference's window-1 loss (the carried-in state held fixed, as the Tape
-    of one window holds it).  CPU only."""
+  * (tests/test_gpu_oracle_real_scene.py, the oracle run on the GPU) the
+    FP64 oracle over two grasp windows with the end-state carry-over of
+    compute_grad (parameter_fitting_functions.py:40-49), and its window-1
+    gradients against central differences of the reference's window-1 loss.
+Here, CPU only: the reference's binary PLY and the scene constants."""
 import json
 import os
 
@@ -71,23 +70,23 @@ def oracle_scene(tree):
     return reference_scene(args, verts, tris, traj, target, mark, op_random, cube_random)
 
 
-def _params(p, grad=False):
+def _params(p, grad=False, device=None):
     names = (("E", 0), ("nu", 1), ("kc", 2), ("ks", 3))    # the golden's order: E, nu, contact, shearing
-    return {k: torch.tensor(float(p[i]), dtype=torch.float64, requires_grad=grad) for k, i in names}
+    return {k: torch.tensor(float(p[i]), dtype=torch.float64, requires_grad=grad, device=device) for k, i in names}
 
 
-def _window(sc, g, init, params, seq):
+def _window(sc, g, init, params, seq, device=None):
     """Window g from initial positions init = (vertices, operator, cube):
     the rollout's states and the loss of compute_loss(max_steps - 2)."""
-    sim, st = OracleSim.initialize(sc["const"], init[0], sc["triangles"], init[1], init[2])
+    sim, st = OracleSim.initialize(sc["const"], init[0], sc["triangles"], init[1], init[2], device=device)
     states = sim64.rollout(sim, st, sc["max_steps"] - 1, params, seq=seq, window=g, keep_states=True)
     loss, _ = sim64.compute_loss(states[sc["max_steps"] - 3]["vx"],
-                                 torch.tensor(sc["targets"][g], dtype=torch.float64))
+                                 torch.tensor(sc["targets"][g], dtype=torch.float64, device=device))
     return states, loss
 
 
 def _end(states):
-    return tuple(states[-1][k].detach().numpy() for k in ("vx", "ox", "cx"))
+    return tuple(states[-1][k].detach().cpu().numpy() for k in ("vx", "ox", "cx"))
 
 
 def test_product_ply_reader_reads_the_reference_binary_mesh(gold, tmp_path):
@@ -121,57 +120,3 @@ def test_product_scene_loader_matches_reference_constants(gold, tree):
     np.testing.assert_allclose(np.asarray(sc.cube_x), gold["cube_model"], rtol=0, atol=1e-15)
     np.testing.assert_allclose(sc.meta["operator_model"], gold["operator_model_without_position"], rtol=0,
                                atol=1e-15)
-
-
-def test_oracle_windows_with_carry_over_match_reference_source(gold, tree):
-    sc = oracle_scene(tree)
-    n_win = int(gold["n_windows"])
-    assert n_win == 2 and sc["max_steps"] == 301
-    params = _params(gold["params"])
-    seq = torch.tensor(sc["grasp_point_pos"], dtype=torch.float64)
-    init = (sc["vertices"], sc["operator_x"], sc["cube_x"])
-    losses = []
-    for g in range(n_win):
-        states, loss = _window(sc, g, init, params, seq)
-        ref = gold["w%d_vertex_x" % g]
-        got = np.stack([s["vx"].numpy() for s in states])
-        err = np.abs(got - ref).max() / np.abs(ref).max()
-        assert err < 2e-4, (g, err)
-        np.testing.assert_allclose(states[-1]["ox"].numpy(), gold["w%d_operator_x_end" % g], rtol=0, atol=1e-5)
-        np.testing.assert_allclose(states[-1]["cx"].numpy(), gold["w%d_cube_x_end" % g], rtol=0, atol=1e-5)
-        assert float(loss) == pytest.approx(float(gold["w%d_loss" % g]), rel=1e-4, abs=0), g
-        losses.append(float(loss))
-        init = _end(states)                       # parameter_fitting_functions.py:40-49
-    assert np.mean(losses) == pytest.approx(float(gold["loss_mean"]), rel=1e-4, abs=0)
-
-
-def test_oracle_window1_gradients_match_reference_finite_differences(tree):
-    g = _load("ref_real_fd_f64.npz")
-    sc = oracle_scene(tree)
-    seq0 = torch.tensor(sc["grasp_point_pos"], dtype=torch.float64)
-    states, loss0 = _window(sc, 0, (sc["vertices"], sc["operator_x"], sc["cube_x"]), _params(g["params"]), seq0)
-    assert float(loss0) == pytest.approx(float(g["w0_loss"]), rel=1e-10, abs=0)
-    np.testing.assert_allclose(states[-1]["vx"].numpy(), g["w0_vertex_x_end"], rtol=0, atol=1e-12)
-    params = _params(g["params"], grad=True)
-    seq = seq0.clone().requires_grad_(True)
-    _, loss = _window(sc, 1, _end(states), params, seq)
-    assert float(loss) == pytest.approx(float(g["w1_loss"]), rel=1e-10, abs=0)
-    loss.backward()
-    L = float(loss)
-    checked = 0
-    for k, key, pv in (("E", "w1_fd_E", 0), ("nu", "w1_fd_nu", 1), ("kc", "w1_fd_contact_stiffness", 2),
-                       ("ks", "w1_fd_shearing_stiffness", 3)):
-        fd = float(g[key])
-        sens = abs(fd) * float(g["params"][pv]) / L
-        if sens < MIN_SENSITIVITY:
-            continue
-        got = float(params[k].grad)
-        assert got == pytest.approx(fd, rel=2e-4, abs=0), (k, got, fd)
-        checked += 1
-    for name in g.files:
-        if name.startswith("w1_fd_seq_"):
-            a, b, c = (int(t) for t in name[len("w1_fd_seq_"):].split("_"))
-            fd = float(g[name])
-            assert fd != 0.0 and float(seq.grad[a, b, c]) == pytest.approx(fd, rel=2e-4, abs=0), name
-            checked += 1
-    assert checked >= 4
