@@ -95,37 +95,48 @@ template <class T> DCP_HD T bspline_dd(int o) { return o == 1 ? T(-2) : T(1); }
 // are evaluated from Ed through exact identities instead:
 //   |f1|^2 - 1 = 2 e1.x + |e1|^2,  f2.f1 = e2.x + e1.y + e1.e2, ...
 //   |h2|^2 - 1 = (|f2|^2 - 1) - r01^2 (2 - |q1|^2), and likewise for h3.
+// Under strong compression a column's squared norm falls towards 0, where
+// 1 + (identity) loses its relative precision and rounding can even make it
+// negative (a NaN under the square root); below 1/4 the squared norm is
+// therefore summed from the column's components, which is never negative.
+// The backward pass differentiates n = sqrt(|h|^2 + eps) through h and does
+// not depend on which form gave the value.
 template <class T> struct QR {
   V3<T> f1, f2, f3, q1, q2, q3, h2, h3;
   T n1, n2, n3, r01, r02, r12;
   T a1, a2, a3;  // n_i - 1
 };
+// n = sqrt(|h|^2 + eps) and a = n - 1 from t = |h|^2 - 1 (small-strain
+// identity) or, when |h|^2 < 1/4, from |h|^2 summed over h's components.
+template <class T> DCP_HD void column_norm(T t, const V3<T>& h, T eps, T& n, T& a) {
+  if (T(1) + t < T(0.25)) {
+    n = sqrt(dot(h, h) + eps);
+    a = n - T(1);
+  } else {
+    n = sqrt(T(1) + (t + eps));
+    a = (t + eps) / (n + T(1));
+  }
+}
 template <class T> DCP_HD void qr_forward(const M3<T>& Ed, QR<T>& s) {
   const T eps = T(1e-9);
   const V3<T> e1 = col(Ed, 0), e2 = col(Ed, 1), e3 = col(Ed, 2);
   s.f1 = v3(T(1) + e1.x, e1.y, e1.z);
   s.f2 = v3(e2.x, T(1) + e2.y, e2.z);
   s.f3 = v3(e3.x, e3.y, T(1) + e3.z);
-  const T s1 = T(2) * e1.x + dot(e1, e1);
-  s.n1 = sqrt(T(1) + (s1 + eps));
-  s.a1 = (s1 + eps) / (s.n1 + T(1));
+  column_norm(T(2) * e1.x + dot(e1, e1), s.f1, eps, s.n1, s.a1);      // |f1|^2 - 1
   s.q1 = s.f1 / s.n1;
   const T q11 = T(1) - eps / (s.n1 * s.n1);           // |q1|^2
   s.r01 = (e2.x + e1.y + dot(e1, e2)) / s.n1;         // f2 . q1
   s.h2 = s.f2 - s.r01 * s.q1;
-  const T t2 = (T(2) * e2.y + dot(e2, e2)) - s.r01 * s.r01 * (T(2) - q11);   // |h2|^2 - 1
-  s.n2 = sqrt(T(1) + (t2 + eps));
-  s.a2 = (t2 + eps) / (s.n2 + T(1));
+  column_norm((T(2) * e2.y + dot(e2, e2)) - s.r01 * s.r01 * (T(2) - q11), s.h2, eps, s.n2, s.a2);  // |h2|^2 - 1
   s.q2 = s.h2 / s.n2;
   const T q22 = T(1) - eps / (s.n2 * s.n2);           // |q2|^2
   const T q12 = s.r01 * (T(1) - q11) / s.n2;          // q1 . q2
   s.r02 = (e3.x + e1.z + dot(e1, e3)) / s.n1;         // f3 . q1
   s.r12 = ((e3.y + e2.z + dot(e2, e3)) - s.r01 * s.r02) / s.n2;   // f3 . q2
   s.h3 = s.f3 - s.r02 * s.q1 - s.r12 * s.q2;
-  const T t3 = (T(2) * e3.z + dot(e3, e3)) - s.r02 * s.r02 * (T(2) - q11) - s.r12 * s.r12 * (T(2) - q22) +
-               T(2) * s.r02 * s.r12 * q12;            // |h3|^2 - 1
-  s.n3 = sqrt(T(1) + (t3 + eps));
-  s.a3 = (t3 + eps) / (s.n3 + T(1));
+  column_norm((T(2) * e3.z + dot(e3, e3)) - s.r02 * s.r02 * (T(2) - q11) - s.r12 * s.r12 * (T(2) - q22) +
+                  T(2) * s.r02 * s.r12 * q12, s.h3, eps, s.n3, s.a3);                     // |h3|^2 - 1
   s.q3 = s.h3 / s.n3;
 }
 // Adjoint of y = h / n with n = sqrt(|h|^2 + eps): returns dL/dh.

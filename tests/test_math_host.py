@@ -173,3 +173,33 @@ def test_float_stress_keeps_precision_at_small_strain(lib, mode):
     lib.h_stress_bwd(n, 0, _p(np.ascontiguousarray(F)), _p(prm), _p(gP), m, _p(gF), _p(gf))
     for j in range(4):
         assert abs(gf[:, j].sum() - gd[:, j].sum()) <= 1e-5 * np.abs(gd[:, j]).sum() + 1e-30, j
+
+
+def test_float_stress_stays_finite_on_nearly_collapsed_columns(lib):
+    """Deformation gradients with one column almost collapsed (|h|^2 far below
+    1, as in a cloth crumpled hard): the float build's QR must sum those squared
+    norms from components (the small-strain identity 1 + (|h|^2 - 1) can round
+    below zero there) and give the double build's stress."""
+    rng = np.random.default_rng(21)
+    F = []
+    for k in range(300):
+        A = np.eye(3) + 0.3 * rng.standard_normal((3, 3))
+        c = k % 3
+        if c == 0:
+            A[:, 0] *= 10.0 ** rng.uniform(-3.5, -1)                           # short first column
+        elif c == 1:
+            A[:, 1] = A[:, 0] * rng.uniform(0.5, 2) + 10.0 ** rng.uniform(-3.5, -1) * rng.standard_normal(3)
+        else:                                                                # third column nearly in-plane
+            A[:, 2] = rng.standard_normal(2) @ A[:, :2].T + 10.0 ** rng.uniform(-3.5, -1) * rng.standard_normal(3)
+        F.append(A)
+    F = np.ascontiguousarray(np.stack(F))
+    n = len(F)
+    prm = np.tile([300.0, 200.0, 100.0, 100.0], (n, 1))
+    P32, P64 = np.zeros((n, 9)), np.zeros((n, 9))
+    lib.h_stress_fwd(n, 0, _p(F), _p(prm), _p(P32))
+    lib.h_stress_fwd(n, 1, _p(F), _p(prm), _p(P64))
+    assert np.isfinite(P32).all()
+    # smallest singular values down to 1e-5: the stress's condition number
+    # reaches 1e5, and float32 keeps a few 1e-3 of it
+    scale = np.abs(P64).max(axis=1)
+    assert (np.abs(P32 - P64).max(axis=1) <= 1e-2 * scale).all()
