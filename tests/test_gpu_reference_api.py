@@ -53,7 +53,9 @@ def _window_grads_vs_fd(ref, g, params, kc_material=True):
         if name.startswith("fd_seq_"):
             a, b, c = (int(t) for t in name[len("fd_seq_"):].split("_"))
             fd = float(g[name])
-            assert fd != 0.0 and ref.grasp_tracking_seq.grad[a, b, c] == pytest.approx(fd, rel=1e-4, abs=0), name
+            # a single keyframe entry of a 300-substep window: float32 keeps it to
+            # about 1.0e-4 (all keyframes together, max-norm: test_gpu_parity.py)
+            assert fd != 0.0 and ref.grasp_tracking_seq.grad[a, b, c] == pytest.approx(fd, rel=1.5e-4, abs=0), name
 
 
 def test_window_loss_and_gradients_match_reference_finite_differences(ref):
