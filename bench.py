@@ -302,7 +302,8 @@ def main():
     else:
         launch = autotune.cached(scenes, info["dt"], cache=cache) if os.path.exists(cache) else None
         launch = launch or dict(autotune.DEFAULT, source="default")
-    batch = ClothBatch(scenes, dt=info["dt"], device=dev, **autotune.batch_kwargs(launch))
+    batch = ClothBatch(scenes, dt=info["dt"], device=dev, pool_blocks=info.get("pool_blocks", 0),
+                       **autotune.batch_kwargs(launch))
     tape = None if args.no_tape else "auto"
     sim = BatchSim(batch, n_steps=info["n_steps"], ckpt_every=info["ckpt_every"], use_graph=True, tape=tape)
     params = batch.params.clone().requires_grad_(True)
@@ -443,7 +444,11 @@ def main():
     if sim._tape is not None:
         meta = ClothBatch.tape_blocks(sim._tape, info["n_steps"])
         tape_info = {"bytes": int(sim._tape.numel()), "substeps_restored": int((meta[:, 0] >= 0).sum()),
-                     "active_blocks_per_substep": float(meta[:, 1].mean())}
+                     "active_blocks_per_substep": float(meta[:, 1].mean()),
+                     "max_active_blocks": int(meta[:, 1].max())}
+    grid_info = {"layout": "paged" if batch.pool_blocks else "dense", "pool_blocks": batch.pool_blocks,
+                 "dense_blocks": int(batch.sizes.total_nodes) // 64,
+                 "grid_bytes": 3 * 16 * 64 * int(batch.sizes.grid_blocks)}
     if rank != 0:
         if world > 1:
             torch.distributed.destroy_process_group()
@@ -454,7 +459,8 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(scenes, info, world),
-        "run": {"launch": launch, "grid_tape": tape_info, "rollout_buffer_gb": sim._buf.numel() * 4 / 1e9,
+        "run": {"launch": launch, "grid": grid_info, "grid_tape": tape_info,
+                "rollout_buffer_gb": sim._buf.numel() * 4 / 1e9,
                 "peak_device_bytes": int(torch.cuda.max_memory_allocated(dev))},
         "roofline": roof,
         "step_roofline": {"achieved": step_alg / (ms_max / 1e3) / 1e9, "unit": "GB/s", "peak": peak,

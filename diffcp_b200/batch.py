@@ -31,17 +31,49 @@ def _stream() -> int:
     return torch.cuda.current_stream().cuda_stream
 
 
+def stencil_blocks(points: np.ndarray, n_grid: int) -> np.ndarray:
+    """Block-major ids of the 4^3-node grid blocks that the quadratic stencils
+    of ``points`` ([n, 3], metres) touch: base cell floor(x / dx - 0.5)
+    (clamped as the kernels clamp it), nodes base .. base + 2 per axis."""
+    pts = np.asarray(points, dtype=np.float64).reshape(-1, 3)
+    base = np.clip(np.floor(pts * n_grid - 0.5), 0, n_grid - 3).astype(np.int64)
+    nb = (n_grid + 3) // 4
+    ids = [(((base + o) >> 2) * np.array([nb * nb, nb, 1])).sum(1)
+           for o in np.array([[i, j, k] for i in (0, 2) for j in (0, 2) for k in (0, 2)])]
+    return np.unique(np.concatenate(ids)) if len(pts) else np.zeros(0, dtype=np.int64)
+
+
+def auto_pool_blocks(scenes: Sequence[ClothScene], margin: float = 4.0) -> int:
+    """Pool size for paged grids: ``margin`` times the blocks that the rest
+    configuration's particles (vertices, triangle centroids, operator and
+    cube particles) touch, plus 256, at most every block of every grid."""
+    touched = sum(len(stencil_blocks(np.concatenate([np.asarray(sc.vertices).reshape(-1, 3),
+                                                     np.asarray(sc.vertices)[np.asarray(sc.triangles)].mean(1),
+                                                     np.asarray(sc.operator_x).reshape(-1, 3),
+                                                     np.asarray(sc.cube_x).reshape(-1, 3)]), sc.n_grid))
+                  for sc in scenes)
+    dense = sum(((sc.n_grid + 3) // 4) ** 3 for sc in scenes)
+    return int(min(dense, int(np.ceil(margin * touched)) + 256))
+
+
 class ClothBatch:
     """Instances of :class:`ClothScene` resident on one GPU.
 
     Particles of each instance are renumbered once into Morton order (a CTA's
     particles then cover a compact grid region); every public method takes and
     returns data in the scenes' original order.
+
+    ``pool_blocks``: 0 keeps every instance's grid dense in memory; an int
+    pages the grids through a pool of that many 4^3-node blocks shared by the
+    batch; "auto" sizes the pool to ``pool_margin`` times the blocks the rest
+    configuration touches (plus 256).  A substep that touches more blocks than
+    the pool holds sets ``native.STATUS_POOL_FULL`` in :meth:`status`.
     """
 
     def __init__(self, scenes: Sequence[ClothScene], dt: float, chunk: int = 128, svd_grad: str = "exact",
                  grid_ctas: int = 0, device=None, reorder: bool = True, scatter_mode: int = 0,
-                 min_blocks: Sequence[int] = (0, 0, 0), adj_scatter_mode: Optional[int] = None):
+                 min_blocks: Sequence[int] = (0, 0, 0), adj_scatter_mode: Optional[int] = None,
+                 pool_blocks=0, pool_margin: float = 4.0):
         self.device = torch.device(device if device is not None else "cuda")
         if self.device.type != "cuda":
             raise ValueError("diffcp_b200 runs on CUDA devices only")
@@ -87,9 +119,13 @@ class ClothBatch:
             I.gripper_radius = sc.gripper_radius
             I.n_traj_steps = 0 if sc.velocities is None else int(sc.velocities.shape[0])
         self._insts = insts
+        if pool_blocks == "auto":
+            pool_blocks = auto_pool_blocks(self.scenes, pool_margin)
+        self.pool_blocks = int(pool_blocks)
         opt = DcpOptions(dt=self.dt, chunk=chunk, svd_grad=native.SVD_GRAD[svd_grad], grid_ctas=grid_ctas,
                          scatter_mode=scatter_mode, min_blocks=(ctypes.c_int32 * 3)(*min_blocks),
-                         adj_scatter_mode=scatter_mode if adj_scatter_mode is None else adj_scatter_mode)
+                         adj_scatter_mode=scatter_mode if adj_scatter_mode is None else adj_scatter_mode,
+                         pool_blocks=self.pool_blocks)
         self._opt = opt
         sizes = DcpSizes()
         check(self.lib.dcp_plan(insts, n, ctypes.byref(opt), ctypes.byref(sizes)), "dcp_plan")

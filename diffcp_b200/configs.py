@@ -125,6 +125,6 @@ def trajectory_batch(seed: int = 0, count: int = 64, n: int = 64, n_steps: int =
 def stress_sheet(seed: int = 0) -> Tuple[List[scene.ClothScene], dict]:
     return [scene.sheet_scene(n=512, side=1.0, height=0.2, n_grid=256, dt=5e-5, n_steps=2000, seed=seed,
                               n_targets=2048, cap_radius=0.8, grasp_amplitude=0.01)], dict(
-        dt=5e-5, n_steps=2000, ckpt_every=45,
-        desc="stress: one cloth 512x512 vertices, 1 m side (bowl-shaped rest, 0.936 m wide), 256^3 grid, dt 5e-5, "
-             "2000 substeps, checkpoints every 45")
+        dt=5e-5, n_steps=2000, ckpt_every=45, pool_blocks="auto",
+        desc="stress: one cloth 512x512 vertices, 1 m side (bowl-shaped rest, 0.936 m wide), 256^3 grid paged "
+             "through a pool of 4^3-node blocks, dt 5e-5, 2000 substeps, checkpoints every 45")

@@ -42,12 +42,14 @@ struct Layout {
   std::vector<Chunk> chunks;
   int n_tri_chunks = 0, n_point_chunks = 0;
   long long nv = 0, nt = 0, no = 0, nc = 0, nq = 0, total_nodes = 0, traj = 0;
+  long long grid_blocks = 0;  // blocks of each grid array (dense: all; paged: pool + spare)
+  int pool_cap = 0;
   int max_nq = 0;
   // static buffer offsets
   size_t off_inst, off_triv, off_chunks, off_rank, static_bytes;
   // workspace offsets
-  size_t off_pm, off_v, off_adj, off_flags, off_lblk, off_linst, off_cnt, off_force, off_contrib, off_barf, off_tmp,
-      off_status, off_qmin, ws_bytes;
+  size_t off_pm, off_v, off_adj, off_flags, off_page, off_lblk, off_linst, off_cnt, off_force, off_contrib, off_barf,
+      off_tmp, off_status, off_qmin, ws_bytes;
 };
 
 int validate(const DcpInstance* in, int n, const DcpOptions* opt) {
@@ -60,6 +62,8 @@ int validate(const DcpInstance* in, int n, const DcpOptions* opt) {
     return fail(DCP_ERR_INVALID, "adj_scatter_mode must be 0, 1 or 2");
   for (int k = 0; k < 3; ++k)
     if (opt->min_blocks[k] < 0 || opt->min_blocks[k] > 4) return fail(DCP_ERR_INVALID, "min_blocks must be 0..4");
+  if (opt->pool_blocks < 0 || opt->pool_blocks > (1 << 24))
+    return fail(DCP_ERR_INVALID, "pool_blocks must be 0..2^24");
   for (int i = 0; i < n; ++i) {
     const DcpInstance& I = in[i];
     char buf[160];
@@ -137,11 +141,16 @@ void make_layout(const DcpInstance* in, int n, const DcpOptions* opt, Layout& L)
   L.off_rank = o; o = align256(o + sizeof(int) * L.nv);
   L.static_bytes = o;
   const long long blocks = L.total_nodes / 64;
+  L.pool_cap = opt->pool_blocks;
+  L.grid_blocks = L.pool_cap > 0 ? L.pool_cap + 1LL : blocks;
+  const long long grid_nodes = 64 * L.grid_blocks;
   o = 0;
-  L.off_pm = o; o = align256(o + 16 * L.total_nodes);
-  L.off_v = o; o = align256(o + 16 * L.total_nodes);
-  L.off_adj = o; o = align256(o + 16 * L.total_nodes);
+  L.off_pm = o; o = align256(o + 16 * grid_nodes);
+  L.off_v = o; o = align256(o + 16 * grid_nodes);
+  L.off_adj = o; o = align256(o + 16 * grid_nodes);
+  // block flags (dense) or page table (paged), one word per block of the batch
   L.off_flags = o; o = align256(o + 4 * blocks);
+  L.off_page = L.off_flags;
   L.off_lblk = o; o = align256(o + 4 * blocks);
   L.off_linst = o; o = align256(o + 4 * blocks);
   L.off_cnt = o; o = align256(o + 64);
@@ -187,6 +196,7 @@ static void fill_sizes(const Layout& L, int n, DcpSizes* s) {
   s->n_tri_chunks = L.n_tri_chunks;
   s->n_point_chunks = L.n_point_chunks;
   s->total_nodes = L.total_nodes;
+  s->grid_blocks = L.grid_blocks;
 }
 
 extern "C" {
@@ -244,6 +254,8 @@ int dcp_create(const DcpInstance* inst, int32_t n_inst, const DcpOptions* opt, c
   cudaStream_t s = (cudaStream_t)stream;
   cudaError_t e = cudaMemcpyAsync(static_dev, host.data(), L.static_bytes, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(workspace_dev, 0, L.ws_bytes, s);
+  if (e == cudaSuccess && L.pool_cap > 0)  // every page entry -1: no block has a slot
+    e = cudaMemsetAsync((unsigned char*)workspace_dev + L.off_page, 0xff, 4 * (size_t)(L.total_nodes / 64), s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
     delete b;
@@ -279,6 +291,8 @@ int dcp_create(const DcpInstance* inst, int32_t n_inst, const DcpOptions* opt, c
   B.qmin = (float*)(wd + L.off_qmin);
   B.total_nodes = L.total_nodes;
   B.total_blocks = L.total_nodes / 64;
+  B.page = L.pool_cap > 0 ? (int*)(wd + L.off_page) : nullptr;
+  B.pool_cap = L.pool_cap;
   b->L.block = opt->chunk;
   // streaming multiprocessors of the current device: the grid-stride kernels
   // launch a multiple of this count

@@ -17,8 +17,13 @@
 // Positions and the triangle's third column are stored relative to the rest
 // configuration so that float32 keeps the small strains that drive the stress
 // (absolute positions near 0.5 would leave ~1e-5 strain resolution).
-//   grid             block-major per instance: 4x4x4-node blocks of 64 nodes,
-//                    float4 (p.xyz, m) / (v_out.xyz, 0) / adjoint per node
+//   grid             4x4x4-node blocks of 64 nodes, float4 (p.xyz, m) /
+//                    (v_out.xyz, 0) / adjoint per node.  Dense: every block of
+//                    every instance's grid, block-major per instance.  Paged:
+//                    a pool of blocks shared by the batch; a page table maps a
+//                    block (instance's first block + block-major index) to its
+//                    pool slot for the current substep, and the slots are the
+//                    positions in the substep's active-block list
 //   topology         [3][Nt] global vertex ids
 #pragma once
 #include <cuda_runtime.h>
@@ -30,7 +35,7 @@ namespace dcp {
 
 enum ChunkKind { CHUNK_VERTEX = 0, CHUNK_OPERATOR = 1, CHUNK_CUBE = 2, CHUNK_TRI = 3 };
 enum GripMode { GRIP_NONE = 0, GRIP_OPERATOR = 1, GRIP_KINEMATIC = 2 };
-enum Status { STATUS_OUT_OF_DOMAIN = 1, STATUS_NONFINITE = 2 };
+enum Status { STATUS_OUT_OF_DOMAIN = 1, STATUS_NONFINITE = 2, STATUS_POOL_FULL = 4 };
 enum GridMode { GRID_FORWARD = 0, GRID_RECOMPUTE = 1 };
 
 // Parameter table row (floats): E, nu, shearing k_s, contact k_c, ground friction, damping.
@@ -81,6 +86,10 @@ struct BatchDev {
   int* status;    // [n_inst]
   float* qmin;    // [nq]
   long long total_nodes, total_blocks;
+  // paged grids (pool_cap > 0): the grid arrays hold pool_cap + 1 blocks, the
+  // last one a spare that absorbs the accesses of blocks without a slot
+  int* page;      // [total_blocks] pool slot of each block, -1 when it has none
+  int pool_cap;   // 0: dense grids
 };
 
 // Floats per particle of a state snapshot and of the rest buffer.
@@ -144,23 +153,79 @@ __device__ __forceinline__ long long node_index(const InstDev& I, int i, int j, 
   return I.node_off + (long long)blk * 64 + within;
 }
 
-// Per-axis parts of the block-major index of a stencil's 27 nodes: node
-// (base + (oi, oj, ok)) of instance I sits at I.node_off + ax[oi] + ay[oj] +
-// az[ok] (the same value as node_index, formed with two adds per node).
-struct NodeOffsets {
+// Addresses of a stencil's 27 nodes: node (base + (oi, oj, ok)) sits at
+// grid_base<PAGED>(grid, I)[at(oi, oj, ok)].
+template <bool PAGED>
+struct StenAddr;
+
+// Dense grids: the block-major index of the node within its instance's grid,
+// formed from per-axis parts with two adds per node (the same value as
+// node_index minus I.node_off).
+template <>
+struct StenAddr<false> {
   int ax[3], ay[3], az[3];
-};
-__device__ __forceinline__ NodeOffsets node_offsets(const InstDev& I, const int base[3]) {
-  NodeOffsets o;
-  const int sy = I.nb * 64, sx = I.nb * sy;
+  __device__ __forceinline__ StenAddr(const BatchDev&, const InstDev& I, const int base[3], bool, int) {
+    const int sy = I.nb * 64, sx = I.nb * sy;
 #pragma unroll
-  for (int q = 0; q < 3; ++q) {
-    const int i = base[0] + q, j = base[1] + q, k = base[2] + q;
-    o.ax[q] = (i >> 2) * sx + ((i & 3) << 4);
-    o.ay[q] = (j >> 2) * sy + ((j & 3) << 2);
-    o.az[q] = ((k >> 2) << 6) + (k & 3);
+    for (int q = 0; q < 3; ++q) {
+      const int i = base[0] + q, j = base[1] + q, k = base[2] + q;
+      ax[q] = (i >> 2) * sx + ((i & 3) << 4);
+      ay[q] = (j >> 2) * sy + ((j & 3) << 2);
+      az[q] = ((k >> 2) << 6) + (k & 3);
+    }
   }
-  return o;
+  __device__ __forceinline__ int at(int oi, int oj, int ok) const { return ax[oi] + ay[oj] + az[ok]; }
+};
+
+// Paged grids: a stencil's 3 nodes per axis span at most 2 blocks per axis
+// (base & 3 >= 2 crosses into the next one), so its 27 nodes lie in at most 8
+// blocks, whose pool slots are looked up once per particle.  A block without
+// a slot (the pool was full when k_alloc claimed it) maps to the spare block
+// and flags the instance with STATUS_POOL_FULL.  Lanes without a particle
+// (valid = false) load nothing.
+template <>
+struct StenAddr<true> {
+  int s[8];  // slot * 64 of block (X, Y, Z) at 4 X + 2 Y + Z (X = 1: the next block along x)
+  int r[3];  // base & 3 per axis
+  __device__ __forceinline__ StenAddr(const BatchDev& B, const InstDev& I, const int base[3], bool valid, int inst) {
+    bool cross[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      r[a] = base[a] & 3;
+      cross[a] = r[a] >= 2;
+    }
+    const int nb = I.nb;
+    const int g0 = (int)(I.node_off >> 6) + ((base[0] >> 2) * nb + (base[1] >> 2)) * nb + (base[2] >> 2);
+    bool bad = false;
+#pragma unroll
+    for (int X = 0; X < 2; ++X)
+#pragma unroll
+      for (int Y = 0; Y < 2; ++Y)
+#pragma unroll
+        for (int Z = 0; Z < 2; ++Z) {
+          int slot = B.pool_cap;
+          if (valid && (X == 0 || cross[0]) && (Y == 0 || cross[1]) && (Z == 0 || cross[2])) {
+            const int q = __ldg(B.page + g0 + (X * nb + Y) * nb + Z);
+            bad = bad || q < 0;
+            slot = q < 0 ? B.pool_cap : q;
+          }
+          s[4 * X + 2 * Y + Z] = slot << 6;
+        }
+    if (bad) atomicOr(B.status + inst, STATUS_POOL_FULL);
+  }
+  __device__ __forceinline__ int at(int oi, int oj, int ok) const {
+    const bool X = oi != 0 && r[0] + oi >= 4, Y = oj != 0 && r[1] + oj >= 4, Z = ok != 0 && r[2] + ok >= 4;
+    const int z0 = Z ? s[1] : s[0], z1 = Z ? s[3] : s[2], z2 = Z ? s[5] : s[4], z3 = Z ? s[7] : s[6];
+    const int y0 = Y ? z1 : z0, y1 = Y ? z3 : z2;
+    return (X ? y1 : y0) + (((r[0] + oi) & 3) << 4) + (((r[1] + oj) & 3) << 2) + ((r[2] + ok) & 3);
+  }
+};
+
+// First node of an instance's grid in a grid array: the instance's offset for
+// dense grids, the pool itself for paged ones.
+template <bool PAGED, class T>
+__device__ __forceinline__ T* grid_base(T* grid, const InstDev& I) {
+  return PAGED ? grid : grid + I.node_off;
 }
 
 // Quadratic B-spline stencil of one particle (simulation.py:140-142): base node
@@ -175,20 +240,23 @@ struct Sten {
   float w[3][3];
   float dw[3][3];
 };
+__device__ __forceinline__ int base_cell(float p, const InstDev& I, bool& bad) {
+  const float t = __fsub_rn(__fmul_rn(p, I.inv_dx), 0.5f);
+  int b = (int)t;
+  if (!(t >= 0.f) || b > I.G - 3) {
+    bad = true;
+    b = b < 0 ? 0 : (b > I.G - 3 ? I.G - 3 : b);
+    if (!(t == t)) b = 0;
+  }
+  return b;
+}
 __device__ __forceinline__ void make_stencil(const float p[3], const InstDev& I, Sten& s, int* status, int inst) {
   bool bad = false;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const float sx = __fmul_rn(p[a], I.inv_dx);
-    const float t = __fsub_rn(sx, 0.5f);
-    int b = (int)t;
-    if (!(t >= 0.f) || b > I.G - 3) {
-      bad = true;
-      b = b < 0 ? 0 : (b > I.G - 3 ? I.G - 3 : b);
-      if (!(t == t)) b = 0;
-    }
+    const int b = base_cell(p[a], I, bad);
     s.base[a] = b;
-    s.fx[a] = __fsub_rn(sx, (float)b);
+    s.fx[a] = __fsub_rn(__fmul_rn(p[a], I.inv_dx), (float)b);
     bspline(s.fx[a], s.w[a], s.dw[a]);
   }
   if (bad) atomicOr(status + inst, STATUS_OUT_OF_DOMAIN);
@@ -223,14 +291,16 @@ __device__ __forceinline__ void mark_block(long long node, unsigned* flags, int*
 // rounds as the longest run needs), mode 1 merges nothing.  Sums are exact
 // float32 additions in a fixed order within the warp.  MARK (P2G) also
 // registers the (at most 8) grid blocks an issuing lane's stencil touches as
-// active.  Every lane of the warp must call it; lanes without a particle pass
-// valid = false.  nz = false declares every contribution of the lane zero
-// (an adjoint particle whose weights vanish): its atomics are skipped.
-template <bool MARK, class F>
+// active on dense grids (k_alloc claims the blocks of paged ones before the
+// substep's P2G).  Every lane of the warp must call it; lanes without a
+// particle pass valid = false.  nz = false declares every contribution of the
+// lane zero (an adjoint particle whose weights vanish): its atomics are skipped.
+template <bool MARK, bool PAGED, class F>
 __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I, int inst, const int base[3],
                                              bool valid, bool nz, F&& contrib) {
   const unsigned FULL = 0xffffffffu;
-  float4* grid = (MARK ? B.grid_pm : B.grid_adj) + I.node_off;
+  constexpr bool MARKS = MARK && !PAGED;
+  float4* grid = grid_base<PAGED>(MARK ? B.grid_pm : B.grid_adj, I);
   const int mode = MARK ? B.scatter_mode : B.adj_scatter_mode;
   if (mode == 2) {
     // pairs: lanes 2i and 2i+1 whose particles share a base cell (neighbours
@@ -245,7 +315,7 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
     const bool theirs = __shfl_xor_sync(FULL, (int)mine, 1) != 0;
     const bool pnz = mine || (pair && theirs);
     const bool issue = valid && (!pair || (lane & 1) == 0);
-    if (MARK && issue) {
+    if (MARKS && issue) {
 #pragma unroll
       for (int bi = 0; bi < 2; ++bi)
 #pragma unroll
@@ -260,7 +330,7 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
           }
     }
     if (!__any_sync(FULL, mine)) return;
-    const NodeOffsets no = node_offsets(I, base);
+    const StenAddr<PAGED> no(B, I, base, issue && pnz, inst);
 #pragma unroll
     for (int oi = 0; oi < 3; ++oi)
 #pragma unroll
@@ -275,13 +345,13 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
             v.x += x; v.y += y; v.z += z;
             if (MARK) v.w += w;
           }
-          if (issue && pnz) atomicAdd(grid + (no.ax[oi] + no.ay[oj] + no.az[ok]), v);
+          if (issue && pnz) atomicAdd(grid + no.at(oi, oj, ok), v);
         }
     return;
   }
   if (mode == 1) {  // per-lane atomics: no shuffles, more L2 traffic
     if (!valid) return;
-    if (MARK) {
+    if (MARKS) {
 #pragma unroll
       for (int bi = 0; bi < 2; ++bi)
 #pragma unroll
@@ -296,13 +366,13 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
           }
     }
     if (!nz) return;
-    const NodeOffsets no = node_offsets(I, base);
+    const StenAddr<PAGED> no(B, I, base, valid, inst);
 #pragma unroll
     for (int oi = 0; oi < 3; ++oi)
 #pragma unroll
       for (int oj = 0; oj < 3; ++oj)
 #pragma unroll
-        for (int ok = 0; ok < 3; ++ok) atomicAdd(grid + (no.ax[oi] + no.ay[oj] + no.az[ok]), contrib(oi, oj, ok));
+        for (int ok = 0; ok < 3; ++ok) atomicAdd(grid + no.at(oi, oj, ok), contrib(oi, oj, ok));
     return;
   }
   const int lane = threadIdx.x & 31;
@@ -322,7 +392,7 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
     const int sg = __shfl_down_sync(FULL, seg, d);
     same[r] = lane + d < 32 && sg == seg;
   }
-  if (MARK && head && valid) {
+  if (MARKS && head && valid) {
 #pragma unroll
     for (int bi = 0; bi < 2; ++bi)
 #pragma unroll
@@ -336,7 +406,7 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
           mark_block(node_index(I, i, j, k), B.flags, B.list_blk, B.list_inst, B.counters, inst);
         }
   }
-  const NodeOffsets no = node_offsets(I, base);
+  const StenAddr<PAGED> no(B, I, base, head && valid, inst);
 #pragma unroll
   for (int oi = 0; oi < 3; ++oi)
 #pragma unroll
@@ -358,7 +428,7 @@ __device__ __forceinline__ void warp_scatter(const BatchDev& B, const InstDev& I
           }
         }
         if (head && valid && (v.x != 0.f || v.y != 0.f || v.z != 0.f || v.w != 0.f))
-          atomicAdd(grid + (no.ax[oi] + no.ay[oj] + no.az[ok]), v);  // (runs check each node: nz unused)
+          atomicAdd(grid + no.at(oi, oj, ok), v);  // (runs check each node: nz unused)
       }
 }
 

@@ -10,7 +10,8 @@ namespace dcp {
 
 enum KernelId {
   KID_TRI_FORWARD = 0, KID_POINT_P2G, KID_GRID, KID_G2P, KID_G2P_ADJ, KID_GRID_ADJ, KID_POINT_ADJ, KID_TRI_ADJ,
-  KID_VERTEX_COLLECT, KID_CHAMFER_FWD, KID_CHAMFER_LOSS, KID_CHAMFER_BWD, KID_INIT, KID_TAPE, KID_RESET, KID_COUNT
+  KID_VERTEX_COLLECT, KID_CHAMFER_FWD, KID_CHAMFER_LOSS, KID_CHAMFER_BWD, KID_INIT, KID_TAPE, KID_RESET, KID_ALLOC,
+  KID_RELEASE, KID_COUNT
 };
 extern const char* const kKernelNames[KID_COUNT];
 

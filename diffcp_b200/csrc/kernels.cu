@@ -196,6 +196,7 @@ __device__ __forceinline__ void lame(float E, float nu, float& mu, float& la) {
 
 // ============================================================== forward
 // One triangle chunk of k_tri_forward.
+template <bool PAGED>
 __device__ __forceinline__ void tri_forward_chunk(const BatchDev& B, const float* __restrict__ params,
                                                   const float* __restrict__ rest, const float* __restrict__ sin,
                                                   const float* __restrict__ fdev, int c) {
@@ -268,7 +269,7 @@ __device__ __forceinline__ void tri_forward_chunk(const BatchDev& B, const float
     }
   }
   // own-node APIC momentum, mass and normal force (simulation.py:250-265)
-  warp_scatter<true>(B, I, ch.inst, st.base, valid, true, [=](int oi, int oj, int ok) -> float4 {
+  warp_scatter<true, PAGED>(B, I, ch.inst, st.base, valid, true, [=](int oi, int oj, int ok) -> float4 {
     const float w0 = st.w[0][oi], w1 = st.w[1][oj], w2 = st.w[2][ok];
     const float w01 = w0 * w1;
     const float W = w01 * w2;
@@ -285,12 +286,12 @@ __device__ __forceinline__ void tri_forward_chunk(const BatchDev& B, const float
 // Triangle P2G.  A full launch has one CTA per chunk; the adjoint substep's
 // launch, which returns at once when the tape holds the substep's grid, has a
 // few CTAs per SM that stride over the chunks otherwise.
-template <int MINB>
+template <int MINB, bool PAGED>
 __global__ void __launch_bounds__(256, MINB) k_tri_forward(BatchDev B, const float* __restrict__ params,
                                                      const float* __restrict__ rest, const float* __restrict__ sin,
                                                      const int2* __restrict__ skip, const float* __restrict__ fdev) {
   if (skip && skip->x >= 0) return;  // the grid of this substep is restored from the tape
-  for (int c = blockIdx.x; c < B.n_tri_chunks; c += gridDim.x) tri_forward_chunk(B, params, rest, sin, fdev, c);
+  for (int c = blockIdx.x; c < B.n_tri_chunks; c += gridDim.x) tri_forward_chunk<PAGED>(B, params, rest, sin, fdev, c);
 }
 
 __device__ __forceinline__ void point_arrays(const BatchDev& B, const StateP& S, int kind, float*& base, long long& n) {
@@ -320,6 +321,7 @@ __device__ __forceinline__ bool operator_velocity(const BatchDev& B, const InstD
 }
 
 // One point chunk (vertex, operator or cube) of k_point_p2g.
+template <bool PAGED>
 __device__ __forceinline__ void point_p2g_chunk(const BatchDev& B, const float* __restrict__ traj, int step,
                                                 int window, const float* __restrict__ rest,
                                                 const float* __restrict__ sin, float* __restrict__ fv_out,
@@ -376,7 +378,7 @@ __device__ __forceinline__ void point_p2g_chunk(const BatchDev& B, const float* 
       K[a] = base_v[a] - (A[3 * a] * st.fx[0] + A[3 * a + 1] * st.fx[1] + A[3 * a + 2] * st.fx[2]);
     }
   }
-  warp_scatter<true>(B, I, ch.inst, st.base, valid, true, [=](int oi, int oj, int ok) -> float4 {
+  warp_scatter<true, PAGED>(B, I, ch.inst, st.base, valid, true, [=](int oi, int oj, int ok) -> float4 {
     const float W = (st.w[0][oi] * st.w[1][oj]) * st.w[2][ok];
     float4 val;
     val.x = W * add_off(add_off(add_off(K[0], oi, A[0]), oj, A[1]), ok, A[2]);
@@ -390,13 +392,94 @@ __device__ __forceinline__ void point_p2g_chunk(const BatchDev& B, const float* 
 }
 
 // Point P2G; launch shapes as for k_tri_forward.
+template <bool PAGED>
 __global__ void __launch_bounds__(256) k_point_p2g(BatchDev B, const float* __restrict__ traj, int step, int window,
                                                    const float* __restrict__ rest, const float* __restrict__ sin,
                                                    const int2* __restrict__ skip, float* __restrict__ fv_out,
                                                    int clear_forces) {
   if (skip && skip->x >= 0) return;  // the grid of this substep is restored from the tape
   for (int c = blockIdx.x; c < B.n_point_chunks; c += gridDim.x)
-    point_p2g_chunk(B, traj, step, window, rest, sin, fv_out, clear_forces, c);
+    point_p2g_chunk<PAGED>(B, traj, step, window, rest, sin, fv_out, clear_forces, c);
+}
+
+// ============================================================== paged grids
+// Claims a pool slot for every block that a particle's stencil touches at
+// the start of the substep: the blocks that P2G, G2P and their adjoints
+// address, found from the same positions by the same base-cell arithmetic.
+// The one thread whose compare-and-swap moves a block's page entry from -1 to
+// -2 takes the next position of the active-block list and stores it as the
+// block's slot; the kernels that read the page table run after this one, so
+// no thread waits for another.  Positions past the pool's capacity get the
+// spare block and flag the instance (STATUS_POOL_FULL); they stay in the list
+// so that k_release clears them.  Lanes whose base cell equals the previous
+// lane's (neighbours in Morton order) skip their claims.  Strides over the
+// chunks like the P2G launches and returns at once when the tape holds the
+// substep (its page entries are restored from the tape by k_grid).
+__global__ void __launch_bounds__(256) k_alloc(BatchDev B, const float* __restrict__ rest,
+                                               const float* __restrict__ sin, const int2* __restrict__ skip) {
+  if (skip && skip->x >= 0) return;
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int n_chunks = B.n_tri_chunks + B.n_point_chunks;
+  StateP S = state_ptrs(const_cast<float*>(sin), B.nv, B.nt, B.no);
+  const RestP R = rest_ptrs(rest, B.nv, B.nt, B.no);
+  for (int c = blockIdx.x; c < n_chunks; c += gridDim.x) {
+    const Chunk ch = B.chunks[c];
+    const InstDev& I = B.inst[ch.inst];
+    const bool valid = threadIdx.x < ch.count;
+    int base[3] = {0, 0, 0};
+    if (valid) {
+      float X[3];
+      if (ch.kind == CHUNK_TRI) {
+        const long long t = ch.start + threadIdx.x, nt = B.nt;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) X[a] = __ldg(S.t + (TRI_XC + a) * nt + t);
+      } else {
+        float* arr;
+        long long n;
+        point_arrays(B, S, ch.kind, arr, n);
+        const float* x0 = point_rest(R, ch.kind);
+        const long long p = ch.start + threadIdx.x;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) X[a] = __ldg(x0 + a * n + p) + __ldg(arr + a * n + p);
+      }
+      bool bad = false;  // flagged by the P2G launches
+#pragma unroll
+      for (int a = 0; a < 3; ++a) base[a] = base_cell(X[a], I, bad);
+    }
+    const int key = valid ? ((base[0] << 22) | (base[1] << 11) | base[2]) : -1 - lane;
+    const int prev = __shfl_up_sync(FULL, key, 1);
+    if (!valid || (lane > 0 && prev == key)) continue;
+    const int nb = I.nb;
+    const int g0 = (int)(I.node_off >> 6) + ((base[0] >> 2) * nb + (base[1] >> 2)) * nb + (base[2] >> 2);
+    const bool cx = (base[0] & 3) >= 2, cy = (base[1] & 3) >= 2, cz = (base[2] & 3) >= 2;
+#pragma unroll
+    for (int X = 0; X < 2; ++X)
+#pragma unroll
+      for (int Y = 0; Y < 2; ++Y)
+#pragma unroll
+        for (int Z = 0; Z < 2; ++Z) {
+          if ((X && !cx) || (Y && !cy) || (Z && !cz)) continue;
+          const int g = g0 + (X * nb + Y) * nb + Z;
+          if (*((volatile int*)(B.page + g)) != -1 || atomicCAS(B.page + g, -1, -2) != -1) continue;
+          const int item = atomicAdd(B.counters, 1);
+          B.list_blk[item] = g;
+          B.list_inst[item] = ch.inst;
+          if (item >= B.pool_cap) atomicOr(B.status + ch.inst, STATUS_POOL_FULL);
+          B.page[g] = item < B.pool_cap ? item : B.pool_cap;
+        }
+  }
+}
+
+// Returns the substep's blocks to the pool: every page entry that k_alloc or
+// the tape restore (k_grid) set is cleared.  GRID_FORWARD: the blocks k_alloc
+// listed; GRID_RECOMPUTE: the tape's list when it holds the substep.
+__global__ void __launch_bounds__(256) k_release(BatchDev B, TapeP T, int step, int mode) {
+  const int2 tm = (mode == GRID_RECOMPUTE && T.meta) ? T.meta[step] : make_int2(-1, 0);
+  const bool from_tape = tm.x >= 0;
+  const int count = from_tape ? min(tm.y, B.pool_cap) : B.counters[0];
+  for (int item = blockIdx.x * blockDim.x + threadIdx.x; item < count; item += gridDim.x * blockDim.x)
+    B.page[from_tape ? __ldg(T.blk + (long long)tm.x + item) : B.list_blk[item]] = -1;
 }
 
 // Node coordinates of lane l (0..63) of an active block.
@@ -433,7 +516,9 @@ __global__ void __launch_bounds__(256) k_grid(BatchDev B, const float* __restric
                                               const float* __restrict__ traj, int step, int mode, TapeP T) {
   const int2 tm = T.meta ? T.meta[step] : make_int2(-1, 0);
   const bool from_tape = mode == GRID_RECOMPUTE && tm.x >= 0;
-  const int count = from_tape ? tm.y : B.counters[0];
+  const bool paged = B.pool_cap > 0;
+  int count = from_tape ? tm.y : B.counters[0];
+  if (paged) count = min(count, B.pool_cap);
   const int record_at = mode == GRID_FORWARD ? tm.x : -1;
   const int per = blockDim.x >> 6, l = threadIdx.x & 63;
   for (int item = blockIdx.x * per + (threadIdx.x >> 6); item < count; item += gridDim.x * per) {
@@ -443,7 +528,10 @@ __global__ void __launch_bounds__(256) k_grid(BatchDev B, const float* __restric
     const InstDev& I = B.inst[inst];
     int i, j, k;
     block_node(I, blk, l, i, j, k);
-    const long long n = (long long)blk * 64 + l;
+    // paged: the pool slot is the list position (the tape's list restores
+    // the page entries of its blocks for the adjoint kernels)
+    const long long n = (paged ? (long long)item : (long long)blk) * 64 + l;
+    if (paged && from_tape && l == 0) B.page[blk] = item;
     const float4 pm = from_tape ? __ldg(T.data + slot * 64 + l) : B.grid_pm[n];
     // the rounded reciprocal: measured faster here than the approximate one
     // that the build selects for divisions (16.5 against 20.2 ms per sweep step)
@@ -467,26 +555,28 @@ __global__ void __launch_bounds__(256) k_grid(BatchDev B, const float* __restric
     }
     if (mode == GRID_FORWARD) {
       B.grid_pm[n] = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (l == 0) B.flags[blk] = 0u;
+      if (!paged && l == 0) B.flags[blk] = 0u;
     } else {
       B.grid_adj[n] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
   }
 }
 
-__device__ __forceinline__ float3 gv_at(const float4* g, const NodeOffsets& o, int oi, int oj, int ok) {
-  const float4 v = __ldg(g + (o.ax[oi] + o.ay[oj] + o.az[ok]));
+template <class A>
+__device__ __forceinline__ float3 gv_at(const float4* g, const A& o, int oi, int oj, int ok) {
+  const float4 v = __ldg(g + o.at(oi, oj, ok));
   return make_float3(v.x, v.y, v.z);
 }
 
 // APIC gather of the grid velocities over a particle's stencil: v = sum W g
 // and C = 4/dx sum W g (x) (o - fx), the latter from the moments
 // mo[a][b] = sum W g_a o_b as C = 4/dx (mo - v fx^T) (o the node's offset
-// 0, 1, 2 per axis).  v may be null.
-__device__ __forceinline__ void gather_affine(const float4* gnb, const InstDev& I, const Sten& st, float inv_dx,
+// 0, 1, 2 per axis).  v may be null.  gnb and nofs address the stencil's
+// nodes (gv_at).
+template <class A>
+__device__ __forceinline__ void gather_affine(const float4* gnb, const A& nofs, const Sten& st, float inv_dx,
                                               float* v_out, float C[9]) {
   float v[3] = {0.f, 0.f, 0.f}, mo[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  const NodeOffsets nofs = node_offsets(I, st.base);
 #pragma unroll
   for (int oi = 0; oi < 3; ++oi)
 #pragma unroll
@@ -518,7 +608,7 @@ __device__ __forceinline__ void gather_affine(const float4* gnb, const InstDev& 
 
 // TRI: launched over the triangle chunks; otherwise over the point chunks
 // (vertex, operator, cube), which follow the triangle chunks in the table.
-template <bool TRI>
+template <bool TRI, bool PAGED>
 __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict__ params,
                                              const float* __restrict__ rest, const float* __restrict__ sin,
                                              float* __restrict__ sout) {
@@ -536,7 +626,8 @@ __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict
     Sten st;
     make_stencil(g.xc, I, st, B.status, ch.inst);
     float Ct[9];
-    gather_affine(B.grid_v + I.node_off, I, st, inv_dx, nullptr, Ct);
+    gather_affine(grid_base<PAGED>(B.grid_v, I), StenAddr<PAGED>(B, I, st.base, true, ch.inst), st, inv_dx,
+                  nullptr, Ct);
     // C = skew + (1 - damping) sym (simulation.py:381-383)
     const float keep = 1.f - __ldg(params + ch.inst * PRM_STRIDE + PRM_DAMPING);
     float Cn[9];
@@ -606,7 +697,7 @@ __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict
   Sten st;
   make_stencil(X, I, st, B.status, ch.inst);
   float v[3], C[9];
-  gather_affine(B.grid_v + I.node_off, I, st, inv_dx, v, C);
+  gather_affine(grid_base<PAGED>(B.grid_v, I), StenAddr<PAGED>(B, I, st.base, true, ch.inst), st, inv_dx, v, C);
   bool finite = true;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
@@ -623,7 +714,7 @@ __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict
 // Reverse of k_g2p: scatter dL/dv_out into the adjoint grid and accumulate
 // the position adjoint of the gather; triangle: reverse of the d3 update and of
 // the skew/sym damping.
-template <int MINB>
+template <int MINB, bool PAGED>
 __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* __restrict__ params,
                                                  const float* __restrict__ rest, const float* __restrict__ sin,
                                                  const float* __restrict__ aout, float* __restrict__ ain,
@@ -692,7 +783,8 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
           for (int b = 0; b < 3; ++b) sym[3 * a + b] = 0.5f * (Cn[3 * a + b] + Cn[3 * b + a]) * ik;
       } else {
         float Ct[9];
-        gather_affine(B.grid_v + I.node_off, I, st, inv_dx, nullptr, Ct);
+        gather_affine(grid_base<PAGED>(B.grid_v, I), StenAddr<PAGED>(B, I, st.base, true, ch.inst), st, inv_dx,
+                      nullptr, Ct);
 #pragma unroll
         for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -780,8 +872,8 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
     for (int a = 0; a < 3; ++a)
 #pragma unroll
       for (int o = 0; o < 3; ++o) ed[a][o] = st.dw[a][o] * inv_dx;
-    const float4* gnb = B.grid_v + I.node_off;
-    const NodeOffsets nofs = node_offsets(I, st.base);
+    const float4* gnb = grid_base<PAGED>(B.grid_v, I);
+    const StenAddr<PAGED> nofs(B, I, st.base, true, ch.inst);
 #pragma unroll
     for (int oi = 0; oi < 3; ++oi)
 #pragma unroll
@@ -827,7 +919,7 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
   for (int a = 0; a < 3; ++a) nz = nz || Kg[a] != 0.f;
 #pragma unroll
   for (int q = 0; q < 9; ++q) nz = nz || cbC[q] != 0.f;
-  warp_scatter<false>(B, I, ch.inst, st.base, valid, nz, [=](int oi, int oj, int ok) -> float4 {
+  warp_scatter<false, PAGED>(B, I, ch.inst, st.base, valid, nz, [=](int oi, int oj, int ok) -> float4 {
     const float W = (st.w[0][oi] * st.w[1][oj]) * st.w[2][ok];
     float4 val;
     val.x = W * add_off(add_off(add_off(Kg[0], oi, cbC[0]), oj, cbC[1]), ok, cbC[2]);
@@ -854,7 +946,9 @@ __global__ void __launch_bounds__(256) k_grid_adj(BatchDev B, const float* __res
                                                   double* __restrict__ gtraj, TapeP T) {
   const int2 tm = T.meta ? T.meta[step] : make_int2(-1, 0);
   const bool from_tape = tm.x >= 0;
-  const int count = from_tape ? tm.y : B.counters[0];
+  const bool paged = B.pool_cap > 0;
+  int count = from_tape ? tm.y : B.counters[0];
+  if (paged) count = min(count, B.pool_cap);
   const int per = blockDim.x >> 6, l = threadIdx.x & 63;
   for (int item = blockIdx.x * per + (threadIdx.x >> 6); item < count; item += gridDim.x * per) {
     const long long slot = (long long)tm.x + item;
@@ -863,7 +957,7 @@ __global__ void __launch_bounds__(256) k_grid_adj(BatchDev B, const float* __res
     const InstDev& I = B.inst[inst];
     int i, j, k;
     block_node(I, blk, l, i, j, k);
-    const long long n = (long long)blk * 64 + l;
+    const long long n = (paged ? (long long)item : (long long)blk) * 64 + l;
     const float4 pm = from_tape ? __ldg(T.data + slot * 64 + l) : B.grid_pm[n];
     const float4 ga = B.grid_adj[n];
     const float inv_m = 1.f / (pm.w + 1e-9f);
@@ -888,9 +982,8 @@ __global__ void __launch_bounds__(256) k_grid_adj(BatchDev B, const float* __res
     B.grid_adj[n] = make_float4(bp[0], bp[1], bp[2], bm);
     if (!from_tape) {
       B.grid_pm[n] = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (l == 0) B.flags[blk] = 0u;
+      if (!paged && l == 0) B.flags[blk] = 0u;
     }
-#pragma unroll
     double gmud = (double)gmu;
     for (int o = 16; o > 0; o >>= 1) gmud += __shfl_xor_sync(0xffffffffu, gmud, o);
     if ((threadIdx.x & 31) == 0 && gmud != 0.0) atomicAdd(gparams + inst * PRM_STRIDE + PRM_FRICTION, gmud);
@@ -898,6 +991,7 @@ __global__ void __launch_bounds__(256) k_grid_adj(BatchDev B, const float* __res
 }
 
 // Reverse of k_point_p2g: gather dL/dp, dL/dm over the stencil.
+template <bool PAGED>
 __global__ void __launch_bounds__(256, 3) k_point_adj(BatchDev B, const float* __restrict__ traj, int step, int window,
                                                    const float* __restrict__ rest, const float* __restrict__ sin,
                                                    float* __restrict__ ain, double* __restrict__ gtraj,
@@ -960,8 +1054,8 @@ __global__ void __launch_bounds__(256, 3) k_point_adj(BatchDev B, const float* _
   float sp[3] = {0.f, 0.f, 0.f};     // sum W bp
   float mo[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // sum W bp (x) o
   float px[3] = {0.f, 0.f, 0.f};
-  const float4* gnb = B.grid_adj + I.node_off;
-  const NodeOffsets nofs = node_offsets(I, st.base);
+  const float4* gnb = grid_base<PAGED>(B.grid_adj, I);
+  const StenAddr<PAGED> nofs(B, I, st.base, true, ch.inst);
 #pragma unroll
   for (int oi = 0; oi < 3; ++oi)
 #pragma unroll
@@ -976,7 +1070,7 @@ __global__ void __launch_bounds__(256, 3) k_point_adj(BatchDev B, const float* _
         const float w2 = st.w[2][ok];
         const float W = w01 * w2;
         const float gW[3] = {e0w1 * w2, w0e1 * w2, w01 * ed[2][ok]};
-        const float4 g = __ldg(gnb + (nofs.ax[oi] + nofs.ay[oj] + nofs.az[ok]));
+        const float4 g = __ldg(gnb + nofs.at(oi, oj, ok));
         const float bp[3] = {g.x, g.y, g.z};
         float s = g.w * m;
 #pragma unroll
@@ -1032,7 +1126,7 @@ __global__ void __launch_bounds__(256, 3) k_point_adj(BatchDev B, const float* _
 // contributions to the three vertices (summed per vertex, added to the vertex
 // adjoint by k_vertex_collect or, inside a rollout, by the next adjoint
 // substep's k_g2p_adj).
-template <int MINB>
+template <int MINB, bool PAGED>
 __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* __restrict__ params,
                                                  const float* __restrict__ rest, const float* __restrict__ sin,
                                                  float* __restrict__ ain, double* __restrict__ gparams) {
@@ -1103,8 +1197,8 @@ __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* 
     float sp[3] = {0.f, 0.f, 0.f}, mo[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     float g3[3] = {0.f, 0.f, 0.f}, sg[3] = {0.f, 0.f, 0.f}, bx[3] = {0.f, 0.f, 0.f};
     float hs[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // (00, 01, 02, 11, 12, 22)
-    const float4* gnb = B.grid_adj + I.node_off;
-    const NodeOffsets nofs = node_offsets(I, st.base);
+    const float4* gnb = grid_base<PAGED>(B.grid_adj, I);
+    const StenAddr<PAGED> nofs(B, I, st.base, true, ch.inst);
 #pragma unroll
     for (int oi = 0; oi < 3; ++oi)
 #pragma unroll
@@ -1121,7 +1215,7 @@ __global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* 
           const float W = w01 * w2;
           const float gW[3] = {e0w1 * w2, w0e1 * w2, w01 * e2};
           const float H[6] = {d0w1 * w2, e0e1 * w2, e0w1 * e2, w0d1 * w2, w0e1 * e2, w01 * ddc[ok]};
-          const float4 ga = __ldg(gnb + (nofs.ax[oi] + nofs.ay[oj] + nofs.az[ok]));
+          const float4 ga = __ldg(gnb + nofs.at(oi, oj, ok));
           const float bp[3] = {ga.x, ga.y, ga.z};
           const float gdot = gW[0] * d3[0] + gW[1] * d3[1] + gW[2] * d3[2];
           const float sP = bp[0] * P3[0] + bp[1] * P3[1] + bp[2] * P3[2];
@@ -1420,7 +1514,7 @@ __global__ void __launch_bounds__(256) k_reset_vertex(BatchDev B, float* __restr
 // Reserve tape slots for the active blocks of substep `step` (one thread).
 __global__ void k_tape_reserve(BatchDev B, TapeP T, int step) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  const int count = B.counters[0];
+  const int count = B.pool_cap > 0 ? min(B.counters[0], B.pool_cap) : B.counters[0];
   const int top = *T.top;
   if ((long long)top + count <= T.cap) {
     T.meta[step] = make_int2(top, count);
@@ -1433,13 +1527,20 @@ __global__ void k_tape_reserve(BatchDev B, TapeP T, int step) {
 // ============================================================== launchers
 const char* const kKernelNames[KID_COUNT] = {
     "k_tri_forward", "k_point_p2g", "k_grid", "k_g2p", "k_g2p_adj", "k_grid_adj", "k_point_adj", "k_tri_adj",
-    "k_vertex_collect", "k_chamfer_fwd", "k_chamfer_loss", "k_chamfer_bwd", "k_init", "k_tape", "k_reset"};
+    "k_vertex_collect", "k_chamfer_fwd", "k_chamfer_loss", "k_chamfer_bwd", "k_init", "k_tape", "k_reset",
+    "k_alloc", "k_release"};
 
 static inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 // Register-cap variants of the three register-heavy kernels: MINB resident
-// 256-thread CTAs per SM (1 = no cap; 4 = 64 registers).
-#define DCP_MINB(kernel, L, i) \
-  (L.min_blocks[i] >= 4 ? kernel<4> : L.min_blocks[i] == 3 ? kernel<3> : (L.min_blocks[i] == 2 ? kernel<2> : kernel<1>))
+// 256-thread CTAs per SM (1 = no cap; 4 = 64 registers), for dense or paged
+// grids.
+#define DCP_MINB_P(kernel, L, i, P)                                                                        \
+  (L.min_blocks[i] >= 4 ? kernel<4, P>                                                                     \
+                        : L.min_blocks[i] == 3 ? kernel<3, P> : (L.min_blocks[i] == 2 ? kernel<2, P> : kernel<1, P>))
+#define DCP_MINB(kernel, L, i) (B.pool_cap > 0 ? DCP_MINB_P(kernel, L, i, true) : DCP_MINB_P(kernel, L, i, false))
+// Dense or paged variant of a kernel template whose last parameter selects it.
+#define DCP_PAGED(kernel, ...) (B.pool_cap > 0 ? kernel<__VA_ARGS__, true> : kernel<__VA_ARGS__, false>)
+#define DCP_PAGED1(kernel) (B.pool_cap > 0 ? kernel<true> : kernel<false>)
 #define DCP_LAUNCH(id, ...)                   \
   do {                                        \
     ProfScope _scope(L.prof, (id), s);        \
@@ -1479,21 +1580,26 @@ cudaError_t launch_forward(const BatchDev& B, const LaunchCfg& L, const float* p
                            int step, int window, const float* sin, float* sout, cudaStream_t s, const TapeP* T,
                            const float* fdev) {
   const TapeP tp = T ? *T : no_tape();
+  const bool paged = B.pool_cap > 0;
+  const int n_chunks = B.n_tri_chunks + B.n_point_chunks;
   cudaMemsetAsync(B.counters, 0, sizeof(int), s);
+  if (paged && n_chunks)
+    DCP_LAUNCH(KID_ALLOC, (k_alloc<<<n_chunks, L.block, 0, s>>>(B, rest, sin, nullptr)));
   if (B.n_tri_chunks)
     DCP_LAUNCH(KID_TRI_FORWARD, (DCP_MINB(k_tri_forward, L, 0)<<<B.n_tri_chunks, L.block, 0, s>>>(
                                     B, params, rest, sin, nullptr, fdev)));
   if (B.n_point_chunks)
-    DCP_LAUNCH(KID_POINT_P2G, (k_point_p2g<<<B.n_point_chunks, L.block, 0, s>>>(
+    DCP_LAUNCH(KID_POINT_P2G, (DCP_PAGED1(k_point_p2g)<<<B.n_point_chunks, L.block, 0, s>>>(
                                   B, traj, step, window, rest, sin, nullptr,
                                   T ? tp.fv + (long long)step * 3 * B.nv : nullptr, 1)));
   if (T) DCP_LAUNCH(KID_TAPE, (k_tape_reserve<<<1, 32, 0, s>>>(B, tp, step)));
   DCP_LAUNCH(KID_GRID, (k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_FORWARD, tp)));
   // points first: the triangle launch forms the next centroids from the vertices' new state
   if (B.n_point_chunks)
-    DCP_LAUNCH(KID_G2P, (k_g2p<false><<<B.n_point_chunks, L.block, 0, s>>>(B, params, rest, sin, sout)));
+    DCP_LAUNCH(KID_G2P, (DCP_PAGED(k_g2p, false)<<<B.n_point_chunks, L.block, 0, s>>>(B, params, rest, sin, sout)));
   if (B.n_tri_chunks)
-    DCP_LAUNCH(KID_G2P, (k_g2p<true><<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin, sout)));
+    DCP_LAUNCH(KID_G2P, (DCP_PAGED(k_g2p, true)<<<B.n_tri_chunks, L.block, 0, s>>>(B, params, rest, sin, sout)));
+  if (paged) DCP_LAUNCH(KID_RELEASE, (k_release<<<L.sm_count * 4, 256, 0, s>>>(B, tp, step, GRID_FORWARD)));
   return cudaGetLastError();
 }
 
@@ -1509,18 +1615,23 @@ cudaError_t launch_backward(const BatchDev& B, const LaunchCfg& L, const float* 
   const int stride_ctas = 2 * L.grid_ctas;
   const int tri_ctas = T && B.n_tri_chunks > stride_ctas ? stride_ctas : B.n_tri_chunks;
   const int point_ctas = T && B.n_point_chunks > stride_ctas ? stride_ctas : B.n_point_chunks;
+  const bool paged = B.pool_cap > 0;
+  const int n_chunks = B.n_tri_chunks + B.n_point_chunks;
+  if (paged && n_chunks)
+    DCP_LAUNCH(KID_ALLOC, (k_alloc<<<T && n_chunks > stride_ctas ? stride_ctas : n_chunks, L.block, 0, s>>>(
+                              B, rest, sin, meta)));
   if (B.n_tri_chunks)
     DCP_LAUNCH(KID_TRI_FORWARD, (DCP_MINB(k_tri_forward, L, 0)<<<tri_ctas, L.block, 0, s>>>(
                                     B, params, rest, sin, meta, nullptr)));
   if (B.n_point_chunks)
-    DCP_LAUNCH(KID_POINT_P2G, (k_point_p2g<<<point_ctas, L.block, 0, s>>>(B, traj, step, window, rest, sin,
-                                                                         meta, nullptr, 0)));
+    DCP_LAUNCH(KID_POINT_P2G, (DCP_PAGED1(k_point_p2g)<<<point_ctas, L.block, 0, s>>>(B, traj, step, window, rest,
+                                                                                    sin, meta, nullptr, 0)));
   DCP_LAUNCH(KID_GRID, (k_grid<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, GRID_RECOMPUTE, tp)));
   DCP_LAUNCH(KID_G2P_ADJ, (DCP_MINB(k_g2p_adj, L, 1)<<<B.n_tri_chunks + B.n_point_chunks, L.block, 0, s>>>(
                               B, params, rest, sin, aout, ain, gparams, snext, fold ? 1 : 0)));
   DCP_LAUNCH(KID_GRID_ADJ, (k_grid_adj<<<L.grid_ctas, 256, 0, s>>>(B, params, traj, step, gparams, gtraj, tp)));
   if (B.n_point_chunks)
-    DCP_LAUNCH(KID_POINT_ADJ, (k_point_adj<<<B.n_point_chunks, L.block, 0, s>>>(
+    DCP_LAUNCH(KID_POINT_ADJ, (DCP_PAGED1(k_point_adj)<<<B.n_point_chunks, L.block, 0, s>>>(
                                   B, traj, step, window, rest, sin, ain, gtraj, meta,
                                   T ? T->fv + (long long)step * 3 * B.nv : nullptr)));
   if (B.n_tri_chunks)
@@ -1528,6 +1639,7 @@ cudaError_t launch_backward(const BatchDev& B, const LaunchCfg& L, const float* 
                                                                                         gparams)));
   if (B.nv && collect)
     DCP_LAUNCH(KID_VERTEX_COLLECT, (k_vertex_collect<<<ceil_div(B.nv, 256), 256, 0, s>>>(B, ain)));
+  if (paged) DCP_LAUNCH(KID_RELEASE, (k_release<<<L.sm_count * 4, 256, 0, s>>>(B, tp, step, GRID_RECOMPUTE)));
   return cudaGetLastError();
 }
 

@@ -21,7 +21,7 @@ DCP_ERR_INVALID = 1
 DCP_ERR_CUDA = 2
 GRIP_NONE, GRIP_OPERATOR, GRIP_KINEMATIC = 0, 1, 2
 SVD_GRAD = {"exact": 0, "reference": 1}
-STATUS_OUT_OF_DOMAIN, STATUS_NONFINITE = 1, 2
+STATUS_OUT_OF_DOMAIN, STATUS_NONFINITE, STATUS_POOL_FULL = 1, 2, 4
 
 EXPORTED = (
     "dcp_plan", "dcp_create", "dcp_destroy", "dcp_sizes", "dcp_init_state", "dcp_substep_forward",
@@ -48,13 +48,14 @@ class DcpInstance(ctypes.Structure):
 class DcpOptions(ctypes.Structure):
     _fields_ = [("dt", c_float), ("chunk", c_int32), ("svd_grad", c_int32), ("grid_ctas", c_int32),
                 ("scatter_mode", c_int32), ("min_blocks", c_int32 * 3),
-                ("adj_scatter_mode", c_int32)]
+                ("adj_scatter_mode", c_int32), ("pool_blocks", c_int32)]
 
 
 class DcpSizes(ctypes.Structure):
     _fields_ = [(n, c_int64) for n in (
         "n_vertex", "n_tri", "n_operator", "n_cube", "n_target", "state_floats", "rest_floats", "traj_floats",
-        "param_floats", "static_bytes", "workspace_bytes", "n_tri_chunks", "n_point_chunks", "total_nodes")]
+        "param_floats", "static_bytes", "workspace_bytes", "n_tri_chunks", "n_point_chunks", "total_nodes",
+        "grid_blocks")]
 
 
 _LIB = None

@@ -67,6 +67,8 @@ extern "C" {
 
 #define DCP_STATUS_OUT_OF_DOMAIN 1 /* a stencil left the grid; clamped */
 #define DCP_STATUS_NONFINITE 2     /* a particle velocity became NaN/Inf, or a Chamfer distance was NaN */
+#define DCP_STATUS_POOL_FULL 4     /* paged grids: a substep touched more blocks than the pool holds; the
+                                      results of that substep are wrong */
 
 /* One cloth scene; the scalars are the constants of src/initialization.py:79,115-130. */
 typedef struct DcpInstance {
@@ -100,6 +102,11 @@ typedef struct DcpOptions {
                            CTAs per SM (1 = none, 2, 3, 4); 0 = default */
   int32_t adj_scatter_mode; /* scatter of the adjoint G2P kernel (k_g2p_adj), same values as
                                scatter_mode, which covers the two P2G kernels */
+  int32_t pool_blocks;  /* 0: dense grids (every 4^3-node block of every instance's grid in memory).
+                           > 0: paged grids, for large sparse ones: a pool of this many blocks shared
+                           by the batch, claimed each substep by the blocks the particles' stencils
+                           touch (sparse grid of the reference's grid_v/grid_m, simulation.py:
+                           274-302); a substep that needs more sets DCP_STATUS_POOL_FULL */
 } DcpOptions;
 
 typedef struct DcpSizes {
@@ -111,6 +118,8 @@ typedef struct DcpSizes {
   int64_t static_bytes;   /* device bytes for topology and launch tables */
   int64_t workspace_bytes;/* device scratch bytes (grids, flags, force buffers) */
   int64_t n_tri_chunks, n_point_chunks, total_nodes;
+  int64_t grid_blocks;    /* 4^3-node blocks held by each grid array: total_nodes / 64 dense,
+                             pool_blocks + 1 (a spare) paged */
 } DcpSizes;
 
 typedef struct DcpBatch DcpBatch;

@@ -35,13 +35,15 @@ def test_struct_layout_matches_c_compiler(tmp_path):
     src = tmp_path / "sz.c"
     src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "%s"\nint main(void){printf("%%zu %%zu %%zu %%zu %%zu\\n",'
                    ' sizeof(DcpInstance), sizeof(DcpOptions), sizeof(DcpSizes), offsetof(DcpInstance, gripper_radius),'
-                   ' offsetof(DcpSizes, total_nodes)); return 0;}\n' % HEADER)
+                   ' offsetof(DcpSizes, total_nodes)); printf("%%zu %%zu\\n", offsetof(DcpOptions, pool_blocks),'
+                   ' offsetof(DcpSizes, grid_blocks)); return 0;}\n' % HEADER)
     exe = tmp_path / "sz"
     subprocess.run(["gcc", "-o", str(exe), str(src)], check=True)
     vals = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
     assert vals == [ctypes.sizeof(native.DcpInstance), ctypes.sizeof(native.DcpOptions),
                     ctypes.sizeof(native.DcpSizes), native.DcpInstance.gripper_radius.offset,
-                    native.DcpSizes.total_nodes.offset]
+                    native.DcpSizes.total_nodes.offset, native.DcpOptions.pool_blocks.offset,
+                    native.DcpSizes.grid_blocks.offset]
 
 
 def _inst(**kw):
@@ -74,3 +76,25 @@ def test_plan_sizes_and_validation():
     assert b"n_operator" in L.dcp_last_error()
     with pytest.raises(native.DcpError):
         native.check(L.dcp_plan(insts2, 1, ctypes.byref(opt), ctypes.byref(s)), "plan")
+
+
+def test_paged_grid_plan_holds_only_the_pool():
+    """pool_blocks > 0: each grid array holds the pool plus one spare block
+    instead of every block of every instance; the dense plan reports all of
+    them.  Out-of-range pool sizes are rejected."""
+    L = native.lib()
+    insts = (native.DcpInstance * 2)(_inst(n_grid=256), _inst(n_grid=64))
+    dense = native.DcpOptions(dt=1e-4, chunk=128, svd_grad=0, grid_ctas=0)
+    paged = native.DcpOptions(dt=1e-4, chunk=128, svd_grad=0, grid_ctas=0, pool_blocks=1000)
+    sd, sp = native.DcpSizes(), native.DcpSizes()
+    assert L.dcp_plan(insts, 2, ctypes.byref(dense), ctypes.byref(sd)) == 0
+    assert L.dcp_plan(insts, 2, ctypes.byref(paged), ctypes.byref(sp)) == 0
+    blocks = 64 ** 3 + 16 ** 3
+    assert sd.total_nodes == sp.total_nodes == 64 * blocks
+    assert sd.grid_blocks == blocks and sp.grid_blocks == 1001
+    # three float4 grid arrays: dense minus paged is their size difference
+    assert sd.workspace_bytes - sp.workspace_bytes >= 3 * 16 * 64 * (blocks - 1001)
+    for bad in (-1, (1 << 24) + 1):
+        opt = native.DcpOptions(dt=1e-4, chunk=128, svd_grad=0, grid_ctas=0, pool_blocks=bad)
+        assert L.dcp_plan(insts, 2, ctypes.byref(opt), ctypes.byref(sp)) == 1
+        assert b"pool_blocks" in L.dcp_last_error()
