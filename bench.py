@@ -47,7 +47,10 @@ KERNEL_BYTES = {
     "k_point_p2g": {"vertex": 88},
     "k_grid": {"node": 48},
     "k_g2p": {"vertex": 84, "tri": 204},
-    "k_g2p_adj": {"vertex": 96, "tri": 144},
+    # vertex_fold: the triangles' per-vertex adjoint sums of the previous
+    # adjoint substep, read and cleared (two float4) in every adjoint substep
+    # of a rollout but its first
+    "k_g2p_adj": {"vertex": 96, "vertex_fold": 64, "tri": 144},
     "k_grid_adj": {"node": 64},
     "k_point_adj": {"vertex": 156},
     "k_tri_adj": {"tri": 372},
@@ -402,7 +405,8 @@ def main():
     batch.profile(False)
     sim.use_graph = True
     n_nodes_active = None
-    units = {"tri": nt, "vertex": nv, "corner": 3 * nt}
+    units = {"tri": nt, "vertex": nv, "corner": 3 * nt,
+             "vertex_fold": nv * (info["n_steps"] - 1) / info["n_steps"]}
     dom = max(prof.items(), key=lambda kv: kv[1][0])
     dname, (dms, dn) = dom
     per_unit = KERNEL_BYTES.get(dname, {})

@@ -304,7 +304,9 @@ int dcp_create(const DcpInstance* inst, int32_t n_inst, const DcpOptions* opt, c
     return cuda_fail(e != cudaSuccess ? e : cudaErrorInvalidValue, "dcp_create: multiprocessor count");
   }
   b->L.sm_count = sms;
-  b->L.grid_ctas = opt->grid_ctas > 0 ? opt->grid_ctas : sms * 8;
+  // k_grid / k_grid_adj are capped to 40 registers (6 resident 256-thread CTAs
+  // per SM): one resident wave of CTAs striding over the active blocks
+  b->L.grid_ctas = opt->grid_ctas > 0 ? opt->grid_ctas : sms * 6;
   const int default_minb[3] = {2, 2, 1};
   for (int k = 0; k < 3; ++k) b->L.min_blocks[k] = opt->min_blocks[k] > 0 ? opt->min_blocks[k] : default_minb[k];
   b->L.prof = &b->prof;

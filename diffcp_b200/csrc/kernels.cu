@@ -512,7 +512,7 @@ __device__ __forceinline__ int kinematic_hit(const InstDev& I, const float* traj
 // reserved it room.  GRID_RECOMPUTE (adjoint substep): when the tape holds this
 // substep's P2G result, reads the active blocks and their (p, m) from the tape
 // in place; otherwise from the P2G this substep recomputed.
-__global__ void __launch_bounds__(256) k_grid(BatchDev B, const float* __restrict__ params,
+__global__ void __launch_bounds__(256, 6) k_grid(BatchDev B, const float* __restrict__ params,
                                               const float* __restrict__ traj, int step, int mode, TapeP T) {
   const int2 tm = T.meta ? T.meta[step] : make_int2(-1, 0);
   const bool from_tape = mode == GRID_RECOMPUTE && tm.x >= 0;
@@ -520,11 +520,24 @@ __global__ void __launch_bounds__(256) k_grid(BatchDev B, const float* __restric
   int count = from_tape ? tm.y : B.counters[0];
   if (paged) count = min(count, B.pool_cap);
   const int record_at = mode == GRID_FORWARD ? tm.x : -1;
-  const int per = blockDim.x >> 6, l = threadIdx.x & 63;
-  for (int item = blockIdx.x * per + (threadIdx.x >> 6); item < count; item += gridDim.x * per) {
-    const long long slot = (long long)tm.x + item;
-    const int blk = from_tape ? __ldg(T.blk + slot) : B.list_blk[item];
-    const int inst = from_tape ? __ldg(T.inst + slot) : B.list_inst[item];
+  const int per = blockDim.x >> 6, l = threadIdx.x & 63, stride = gridDim.x * per;
+  // the block id, instance and (p, m) of a list item; the next item's are
+  // loaded before the current one is processed (its loads do not depend on
+  // the current item's stores: every item is a different block)
+  auto fetch = [&](int it, int& blk, int& inst, float4& pm) {
+    const long long slot = (long long)tm.x + it;
+    blk = from_tape ? __ldg(T.blk + slot) : B.list_blk[it];
+    inst = from_tape ? __ldg(T.inst + slot) : B.list_inst[it];
+    pm = from_tape ? __ldg(T.data + slot * 64 + l) : B.grid_pm[(paged ? (long long)it : (long long)blk) * 64 + l];
+  };
+  int item = blockIdx.x * per + (threadIdx.x >> 6);
+  int blk = 0, inst = 0;
+  float4 pm = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (item < count) fetch(item, blk, inst, pm);
+  for (; item < count; item += stride) {
+    int blk_n = 0, inst_n = 0;
+    float4 pm_n = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (item + stride < count) fetch(item + stride, blk_n, inst_n, pm_n);
     const InstDev& I = B.inst[inst];
     int i, j, k;
     block_node(I, blk, l, i, j, k);
@@ -532,7 +545,6 @@ __global__ void __launch_bounds__(256) k_grid(BatchDev B, const float* __restric
     // the page entries of its blocks for the adjoint kernels)
     const long long n = (paged ? (long long)item : (long long)blk) * 64 + l;
     if (paged && from_tape && l == 0) B.page[blk] = item;
-    const float4 pm = from_tape ? __ldg(T.data + slot * 64 + l) : B.grid_pm[n];
     // the rounded reciprocal: measured faster here than the approximate one
     // that the build selects for divisions (16.5 against 20.2 ms per sweep step)
     const float inv_m = __frcp_rn(pm.w + 1e-9f);
@@ -559,6 +571,9 @@ __global__ void __launch_bounds__(256) k_grid(BatchDev B, const float* __restric
     } else {
       B.grid_adj[n] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
+    blk = blk_n;
+    inst = inst_n;
+    pm = pm_n;
   }
 }
 
@@ -941,7 +956,7 @@ __global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* 
 // active blocks and their (p, m) come from the tape when it holds this
 // substep (as in k_grid), otherwise from this substep's recomputed P2G, whose
 // grid and block flags are cleared here for the next substep.
-__global__ void __launch_bounds__(256) k_grid_adj(BatchDev B, const float* __restrict__ params,
+__global__ void __launch_bounds__(256, 6) k_grid_adj(BatchDev B, const float* __restrict__ params,
                                                   const float* __restrict__ traj, int step, double* __restrict__ gparams,
                                                   double* __restrict__ gtraj, TapeP T) {
   const int2 tm = T.meta ? T.meta[step] : make_int2(-1, 0);
@@ -949,17 +964,29 @@ __global__ void __launch_bounds__(256) k_grid_adj(BatchDev B, const float* __res
   const bool paged = B.pool_cap > 0;
   int count = from_tape ? tm.y : B.counters[0];
   if (paged) count = min(count, B.pool_cap);
-  const int per = blockDim.x >> 6, l = threadIdx.x & 63;
-  for (int item = blockIdx.x * per + (threadIdx.x >> 6); item < count; item += gridDim.x * per) {
-    const long long slot = (long long)tm.x + item;
-    const int blk = from_tape ? __ldg(T.blk + slot) : B.list_blk[item];
-    const int inst = from_tape ? __ldg(T.inst + slot) : B.list_inst[item];
+  const int per = blockDim.x >> 6, l = threadIdx.x & 63, stride = gridDim.x * per;
+  // the next item's loads are issued before the current item is processed
+  // (every item is a different block, so they do not depend on its stores)
+  auto fetch = [&](int it, int& blk, int& inst, float4& pm, float4& ga) {
+    const long long slot = (long long)tm.x + it;
+    blk = from_tape ? __ldg(T.blk + slot) : B.list_blk[it];
+    inst = from_tape ? __ldg(T.inst + slot) : B.list_inst[it];
+    const long long n = (paged ? (long long)it : (long long)blk) * 64 + l;
+    pm = from_tape ? __ldg(T.data + slot * 64 + l) : B.grid_pm[n];
+    ga = B.grid_adj[n];
+  };
+  int item = blockIdx.x * per + (threadIdx.x >> 6);
+  int blk = 0, inst = 0;
+  float4 pm = make_float4(0.f, 0.f, 0.f, 0.f), ga = pm;
+  if (item < count) fetch(item, blk, inst, pm, ga);
+  for (; item < count; item += stride) {
+    int blk_n = 0, inst_n = 0;
+    float4 pm_n = make_float4(0.f, 0.f, 0.f, 0.f), ga_n = pm_n;
+    if (item + stride < count) fetch(item + stride, blk_n, inst_n, pm_n, ga_n);
     const InstDev& I = B.inst[inst];
     int i, j, k;
     block_node(I, blk, l, i, j, k);
     const long long n = (paged ? (long long)item : (long long)blk) * 64 + l;
-    const float4 pm = from_tape ? __ldg(T.data + slot * 64 + l) : B.grid_pm[n];
-    const float4 ga = B.grid_adj[n];
     const float inv_m = 1.f / (pm.w + 1e-9f);
     const float v[3] = {inv_m * pm.x, inv_m * pm.y, inv_m * pm.z};
     const float mu_g = __ldg(params + inst * PRM_STRIDE + PRM_FRICTION);
@@ -987,6 +1014,10 @@ __global__ void __launch_bounds__(256) k_grid_adj(BatchDev B, const float* __res
     double gmud = (double)gmu;
     for (int o = 16; o > 0; o >>= 1) gmud += __shfl_xor_sync(0xffffffffu, gmud, o);
     if ((threadIdx.x & 31) == 0 && gmud != 0.0) atomicAdd(gparams + inst * PRM_STRIDE + PRM_FRICTION, gmud);
+    blk = blk_n;
+    inst = inst_n;
+    pm = pm_n;
+    ga = ga_n;
   }
 }
 
