@@ -42,8 +42,9 @@ Outputs
   ref_real_fd_f64.npz   the same scene in float64: window 0, the carry-over,
                         and central finite differences of the window-1 loss
                         with respect to E, nu, contact/shearing stiffness and
-                        two grasp-trajectory coordinates, the carried-in state
-                        held fixed (the Tape of compute_grad covers one window)
+                        three horizontal grasp-trajectory coordinates (two
+                        step sizes each), the carried-in state held fixed (the
+                        Tape of compute_grad covers one window)
 
 Run:  python tests/golden/make_golden.py --ref PATH   (PATH: the reference's
 source tree; or set DIFFCP_REFERENCE)
@@ -103,11 +104,18 @@ PARAMS_PRESS = {"E": 400.0, "nu": 0.3, "contact_stiffness": 1000.0, "shearing_st
 # moves the grippers from frame g to g + 1), frames 0..3 of the grasp
 # trajectory (end_frame 3) and the first REAL_WINDOWS target windows; the other
 # keys are those of the reference's simulation_arguments.json.  Window 1's
-# loss depends on keyframes 1 and 2 (REAL_SEQ_COORDS).
+# loss depends on keyframes 1 and 2 (REAL_SEQ_COORDS).  Frames 1-3 of the
+# trajectory coincide, so the grippers rest through window 1 and the loss has
+# a kink in every keyframe's height (y): a gripper velocity up or down moves
+# the sheet against the floor differently.  The differences therefore run
+# along horizontal coordinates (x: 0, z: 2), each with two steps
+# (REAL_SEQ_STEPS); tests compare a gradient with them only where the two
+# agree.
 REAL_OVERRIDES = {"grad_update_interval": 0.03001, "end_frame": 3}
 REAL_WINDOWS = 2
 REAL_FRAMES = 4
-REAL_SEQ_COORDS = ((1, 0, 1), (2, 1, 0))
+REAL_SEQ_COORDS = ((1, 0, 2), (2, 1, 0), (2, 0, 0))
+REAL_SEQ_STEPS = (1e-7, 1e-6)
 REAL_HISTORY_STRIDE = 10   # vertex histories of ref_real_f32.npz: every 10th substep
 REAL_WORKERS = 6
 
@@ -485,11 +493,11 @@ def run_real64(tree, out):
             p[name] = base[name] + sgn * rel_h * base[name]
             tasks.append((p, None))
             keys.append(("param", name, sgn))
-    h_seq = 1e-7
-    for coord in REAL_SEQ_COORDS:
-        for sgn in (1, -1):
-            tasks.append((dict(base), (coord, sgn * h_seq)))
-            keys.append(("seq", coord, sgn))
+    for h_seq in REAL_SEQ_STEPS:
+        for coord in REAL_SEQ_COORDS:
+            for sgn in (1, -1):
+                tasks.append((dict(base), (coord, sgn * h_seq)))
+                keys.append(("seq", coord, sgn, h_seq))
     ctx = multiprocessing.get_context("spawn")
     with concurrent.futures.ProcessPoolExecutor(REAL_WORKERS, mp_context=ctx, initializer=_real64_worker,
                                                 initargs=(tree, carried_path)) as ex:
@@ -500,8 +508,11 @@ def run_real64(tree, out):
     for name in ("E", "nu", "contact_stiffness", "shearing_stiffness"):
         h = rel_h * base[name]
         rec["w1_fd_" + name] = (res[("param", name, 1)] - res[("param", name, -1)]) / (2 * h)
-    for coord in REAL_SEQ_COORDS:
-        rec["w1_fd_seq_%d_%d_%d" % coord] = (res[("seq", coord, 1)] - res[("seq", coord, -1)]) / (2 * h_seq)
+    # w1_fd_seq_*: step REAL_SEQ_STEPS[0]; w1_fd2_seq_*: step REAL_SEQ_STEPS[1]
+    for prefix, h_seq in zip(("w1_fd_seq_", "w1_fd2_seq_"), REAL_SEQ_STEPS):
+        for coord in REAL_SEQ_COORDS:
+            rec[prefix + "%d_%d_%d" % coord] = (res[("seq", coord, 1, h_seq)] - res[("seq", coord, -1, h_seq)]) / (
+                2 * h_seq)
     rec["params"] = np.array([base["E"], base["nu"], base["contact_stiffness"], base["shearing_stiffness"]])
     rec["max_steps"] = np.array(m.max_steps)
     np.savez_compressed(out, **rec)

@@ -16,7 +16,8 @@ import torch
 
 from tests.golden import make_golden as mg
 from tests.ref_tree import write_real_tree
-from tests.test_oracle_real_scene import MIN_SENSITIVITY, _end, _load, _params, _window, oracle_scene
+from tests.test_oracle_real_scene import (MIN_SENSITIVITY, _end, _load, _params, _window, oracle_scene,
+                                          resolved_seq_differences)
 
 pytestmark = pytest.mark.gpu
 
@@ -81,10 +82,7 @@ def test_oracle_window1_gradients_match_reference_finite_differences(tree):
         got = float(params[k].grad)
         assert got == pytest.approx(fd, rel=2e-4, abs=0), (k, got, fd)
         checked += 1
-    for name in g.files:
-        if name.startswith("w1_fd_seq_"):
-            a, b, c = (int(t) for t in name[len("w1_fd_seq_"):].split("_"))
-            fd = float(g[name])
-            assert fd != 0.0 and float(seq.grad[a, b, c]) == pytest.approx(fd, rel=2e-4, abs=0), name
-            checked += 1
+    for a, b, c, fd in resolved_seq_differences(g):
+        assert float(seq.grad[a, b, c]) == pytest.approx(fd, rel=2e-4, abs=0), (a, b, c)
+        checked += 1
     assert checked >= 2

@@ -35,6 +35,39 @@ GOLD = os.path.join(os.path.dirname(__file__), "golden")
 MIN_SENSITIVITY = 5e-6
 
 
+# Two central differences of a keyframe coordinate (steps 1e-7 and 1e-6 of
+# make_golden.REAL_SEQ_STEPS) that differ by more than this, relative, mark a
+# coordinate where the loss is not smooth at the scale of the step; a
+# gradient is compared with a difference only where the two agree.
+SEQ_STEP_AGREEMENT = 2e-5
+
+
+def resolved_seq_differences(fd):
+    """(keyframe, grasp, axis, difference) of every trajectory coordinate of
+    ref_real_fd_f64.npz whose two step sizes agree; asserts that the fixture
+    holds at least two such coordinates."""
+    out = []
+    for name in fd.files:
+        if not name.startswith("w1_fd_seq_"):
+            continue
+        key = name[len("w1_fd_seq_"):]
+        a, b, c = (int(t) for t in key.split("_"))
+        d1, d2 = float(fd[name]), float(fd["w1_fd2_seq_" + key])
+        assert d1 != 0.0, name
+        if abs(d1 - d2) <= SEQ_STEP_AGREEMENT * abs(d1):
+            out.append((a, b, c, d1))
+    assert len(out) >= 2, "fewer than two resolved keyframe differences"
+    return out
+
+
+def test_keyframe_differences_are_resolved():
+    """The golden keyframe differences are taken where the window-1 loss is
+    smooth: both step sizes give the same difference."""
+    fd = _load("ref_real_fd_f64.npz")
+    res = resolved_seq_differences(fd)
+    assert len(res) == sum(1 for n in fd.files if n.startswith("w1_fd_seq_"))
+
+
 def _load(name):
     path = os.path.join(GOLD, name)
     if not os.path.exists(path):
