@@ -137,15 +137,38 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel):
-    """DRAM read + write bytes of one launch of ``kernel`` on this workload,
-    from the committed ncu summary (profiles/<kernel>.md, line
-    'dram_bytes_per_launch: X'); None when no summary exists."""
+def ncu_figure(kernel, key):
+    """A per-launch figure of ``kernel`` on this workload from its committed
+    ncu summary (profiles/<kernel>.md, line '<key>: X'); None when absent."""
     path = os.path.join(ROOT, "profiles", kernel + ".md")
     if not os.path.exists(path):
         return None
-    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+-]+)", open(path).read())
+    m = re.search(key + r":\s*([0-9.eE+-]+)", open(path).read())
     return float(m.group(1)) if m else None
+
+
+def ncu_traffic(kernel):
+    """DRAM read + write bytes of one launch of ``kernel``
+    ('dram_bytes_per_launch')."""
+    return ncu_figure(kernel, "dram_bytes_per_launch")
+
+
+def issue_ceiling(kernel, avg_launch_s, sm_mhz):
+    """The kernel's instruction-issue rate against the SMs' issue ceiling (one
+    warp instruction per cycle on each of an SM's 4 schedulers) at the SM
+    clock sampled under load: the stencil kernels are bound by issue and
+    latency, not by HBM, and this says how far from that ceiling they run.
+    Warp instructions per launch come from the ncu summary
+    ('warp_inst_per_launch'); None when absent."""
+    import torch
+    inst = ncu_figure(kernel, "warp_inst_per_launch")
+    if inst is None or not sm_mhz:
+        return None
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    peak = 4.0 * sms * sm_mhz * 1e6
+    achieved = inst / avg_launch_s
+    return {"kernel": kernel, "achieved": achieved, "peak": peak, "unit": "warp instructions/s",
+            "frac": achieved / peak, "warp_inst_per_launch": inst, "sms": sms, "sm_mhz": sm_mhz}
 
 
 def counts(scenes):
@@ -458,6 +481,7 @@ def main():
             torch.distributed.destroy_process_group()
         return
     cpu = None if args.no_cpu or world > 1 else cpu_rate(scenes, info, seconds=args.cpu_seconds)
+    clocks = clk.summary()
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
@@ -467,6 +491,7 @@ def main():
                 "rollout_buffer_gb": sim._buf.numel() * 4 / 1e9,
                 "peak_device_bytes": int(torch.cuda.max_memory_allocated(dev))},
         "roofline": roof,
+        "issue_roofline": issue_ceiling(dname, dms / dn / 1e3, clocks.get("sm_mhz")),
         "step_roofline": {"achieved": step_alg / (ms_max / 1e3) / 1e9, "unit": "GB/s", "peak": peak,
                           "frac": step_alg / (ms_max / 1e3) / 1e9 / peak,
                           "bytes_per_particle": STEP_BYTES},
@@ -477,7 +502,7 @@ def main():
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": ms_e2e_max},
         "gpu_launches": int(launches),
-        "clocks": clk.summary(),
+        "clocks": clocks,
         "status_nonzero_instances": int((status != 0).sum()),
         "nonfinite_instances": int(((status & 2) != 0).sum()),
     }

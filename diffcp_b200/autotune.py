@@ -8,8 +8,9 @@ workload on the device:
                      the two P2G kernels, and ``adj_scatter_mode`` likewise
                      for the adjoint G2P kernel, each from its own kernels'
                      CUDA-event times,
-  * ``min_blocks``   the register cap of each register-heavy kernel
-                     (k_tri_forward, k_g2p_adj, k_tri_adj), chosen per kernel
+  * ``min_blocks``   the register-cap level of each register-heavy kernel
+                     (k_tri_forward, k_g2p_adj, k_tri_adj; 1 none, 2 128,
+                     3 96, 4 80, 5 72, 6 64 registers), chosen per kernel
                      from the per-kernel CUDA-event times of one run per level.
 Results are cached per workload signature in ``tuned.json`` next to this
 file (or a path given by the caller).
@@ -32,6 +33,7 @@ HEAVY = ("k_tri_forward", "k_g2p_adj", "k_tri_adj")
 P2G = ("k_tri_forward", "k_point_p2g")
 ADJ = ("k_g2p_adj",)
 DEFAULT = {"chunk": 128, "scatter_mode": 0, "adj_scatter_mode": 0, "min_blocks": [2, 2, 1]}
+LEVELS = (1, 2, 3, 4, 5, 6)   # register-cap levels (DcpOptions.min_blocks)
 
 
 def batch_kwargs(cfg: dict) -> dict:
@@ -110,14 +112,14 @@ def tune(scenes: Sequence[ClothScene], dt: float, substeps: int = 3, device=None
     runs.sort(key=lambda r: r[0])
     _, chunk, mode, adj_mode = runs[0]
     per_level = {}
-    for level in (1, 2, 3, 4):
+    for level in LEVELS:
         b = ClothBatch(scenes, dt=dt, chunk=chunk, scatter_mode=mode, adj_scatter_mode=adj_mode,
                        min_blocks=(level,) * 3, device=device)
         _time_substeps(b, 1)
         per_level[level] = _time_substeps(b, substeps)
         b.close()
         del b
-    mb = [min((1, 2, 3, 4), key=lambda lv: per_level[lv].get(k, float("inf"))) for k in HEAVY]
+    mb = [min(LEVELS, key=lambda lv: per_level[lv].get(k, float("inf"))) for k in HEAVY]
     cfg = {"chunk": chunk, "scatter_mode": mode, "adj_scatter_mode": adj_mode, "min_blocks": mb}
     if verbose:
         for lv, t in per_level.items():

@@ -61,7 +61,7 @@ int validate(const DcpInstance* in, int n, const DcpOptions* opt) {
   if (opt->adj_scatter_mode < 0 || opt->adj_scatter_mode > 2)
     return fail(DCP_ERR_INVALID, "adj_scatter_mode must be 0, 1 or 2");
   for (int k = 0; k < 3; ++k)
-    if (opt->min_blocks[k] < 0 || opt->min_blocks[k] > 4) return fail(DCP_ERR_INVALID, "min_blocks must be 0..4");
+    if (opt->min_blocks[k] < 0 || opt->min_blocks[k] > 6) return fail(DCP_ERR_INVALID, "min_blocks must be 0..6");
   if (opt->pool_blocks < 0 || opt->pool_blocks > (1 << 24))
     return fail(DCP_ERR_INVALID, "pool_blocks must be 0..2^24");
   for (int i = 0; i < n; ++i) {

@@ -65,7 +65,7 @@ struct LaunchCfg {
   int block;      // threads per CTA = particles per chunk
   int grid_ctas;  // CTAs of the persistent grid-update kernels
   int sm_count = 0;   // multiprocessors of the batch's device (dcp_create queries it)
-  int min_blocks[3] = {2, 2, 1};  // register caps of k_tri_forward, k_g2p_adj, k_tri_adj (1..3)
+  int min_blocks[3] = {2, 2, 1};  // register-cap levels of k_tri_forward, k_g2p_adj, k_tri_adj (1..6)
   Profiler* prof = nullptr;
 };
 

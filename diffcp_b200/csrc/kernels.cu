@@ -286,8 +286,8 @@ __device__ __forceinline__ void tri_forward_chunk(const BatchDev& B, const float
 // Triangle P2G.  A full launch has one CTA per chunk; the adjoint substep's
 // launch, which returns at once when the tape holds the substep's grid, has a
 // few CTAs per SM that stride over the chunks otherwise.
-template <int MINB, bool PAGED>
-__global__ void __launch_bounds__(256, MINB) k_tri_forward(BatchDev B, const float* __restrict__ params,
+template <int REGS, bool PAGED>
+__global__ void __maxnreg__(REGS) k_tri_forward(BatchDev B, const float* __restrict__ params,
                                                      const float* __restrict__ rest, const float* __restrict__ sin,
                                                      const int2* __restrict__ skip, const float* __restrict__ fdev) {
   if (skip && skip->x >= 0) return;  // the grid of this substep is restored from the tape
@@ -391,9 +391,11 @@ __device__ __forceinline__ void point_p2g_chunk(const BatchDev& B, const float* 
   if (clear_forces && valid && ch.kind == CHUNK_VERTEX) B.fvert[p] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
-// Point P2G; launch shapes as for k_tri_forward.
+// Point P2G; launch shapes as for k_tri_forward.  Capped at 56 registers on
+// dense grids (no spills; measured faster than the uncapped 62), 80 on paged
+// ones (their stencil addressing needs the slots of up to 8 blocks).
 template <bool PAGED>
-__global__ void __launch_bounds__(256) k_point_p2g(BatchDev B, const float* __restrict__ traj, int step, int window,
+__global__ void __maxnreg__(PAGED ? 80 : 56) k_point_p2g(BatchDev B, const float* __restrict__ traj, int step, int window,
                                                    const float* __restrict__ rest, const float* __restrict__ sin,
                                                    const int2* __restrict__ skip, float* __restrict__ fv_out,
                                                    int clear_forces) {
@@ -729,8 +731,8 @@ __global__ void __launch_bounds__(256) k_g2p(BatchDev B, const float* __restrict
 // Reverse of k_g2p: scatter dL/dv_out into the adjoint grid and accumulate
 // the position adjoint of the gather; triangle: reverse of the d3 update and of
 // the skew/sym damping.
-template <int MINB, bool PAGED>
-__global__ void __launch_bounds__(256, MINB) k_g2p_adj(BatchDev B, const float* __restrict__ params,
+template <int REGS, bool PAGED>
+__global__ void __maxnreg__(REGS) k_g2p_adj(BatchDev B, const float* __restrict__ params,
                                                  const float* __restrict__ rest, const float* __restrict__ sin,
                                                  const float* __restrict__ aout, float* __restrict__ ain,
                                                  double* __restrict__ gparams, const float* __restrict__ snext,
@@ -1023,7 +1025,7 @@ __global__ void __launch_bounds__(256, 6) k_grid_adj(BatchDev B, const float* __
 
 // Reverse of k_point_p2g: gather dL/dp, dL/dm over the stencil.
 template <bool PAGED>
-__global__ void __launch_bounds__(256, 3) k_point_adj(BatchDev B, const float* __restrict__ traj, int step, int window,
+__global__ void __launch_bounds__(256, 4) k_point_adj(BatchDev B, const float* __restrict__ traj, int step, int window,
                                                    const float* __restrict__ rest, const float* __restrict__ sin,
                                                    float* __restrict__ ain, double* __restrict__ gtraj,
                                                    const int2* __restrict__ tmeta, const float* __restrict__ fv_in) {
@@ -1157,8 +1159,8 @@ __global__ void __launch_bounds__(256, 3) k_point_adj(BatchDev B, const float* _
 // contributions to the three vertices (summed per vertex, added to the vertex
 // adjoint by k_vertex_collect or, inside a rollout, by the next adjoint
 // substep's k_g2p_adj).
-template <int MINB, bool PAGED>
-__global__ void __launch_bounds__(256, MINB) k_tri_adj(BatchDev B, const float* __restrict__ params,
+template <int REGS, bool PAGED>
+__global__ void __maxnreg__(REGS) k_tri_adj(BatchDev B, const float* __restrict__ params,
                                                  const float* __restrict__ rest, const float* __restrict__ sin,
                                                  float* __restrict__ ain, double* __restrict__ gparams) {
   const Chunk ch = B.chunks[blockIdx.x];
@@ -1562,12 +1564,16 @@ const char* const kKernelNames[KID_COUNT] = {
     "k_alloc", "k_release"};
 
 static inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
-// Register-cap variants of the three register-heavy kernels: MINB resident
-// 256-thread CTAs per SM (1 = no cap; 4 = 64 registers), for dense or paged
-// grids.
-#define DCP_MINB_P(kernel, L, i, P)                                                                        \
-  (L.min_blocks[i] >= 4 ? kernel<4, P>                                                                     \
-                        : L.min_blocks[i] == 3 ? kernel<3, P> : (L.min_blocks[i] == 2 ? kernel<2, P> : kernel<1, P>))
+// Register-cap variants of the three register-heavy kernels, by level:
+// 1 = no cap (255 registers), 2 = 128, 3 = 96, 4 = 80, 5 = 72, 6 = 64; for
+// dense or paged grids.  A cap trades spills for resident warps.
+#define DCP_MINB_P(kernel, L, i, P)                                                                     \
+  (L.min_blocks[i] >= 6   ? kernel<64, P>                                                               \
+   : L.min_blocks[i] == 5 ? kernel<72, P>                                                               \
+   : L.min_blocks[i] == 4 ? kernel<80, P>                                                               \
+   : L.min_blocks[i] == 3 ? kernel<96, P>                                                               \
+   : L.min_blocks[i] == 2 ? kernel<128, P>                                                              \
+                          : kernel<255, P>)
 #define DCP_MINB(kernel, L, i) (B.pool_cap > 0 ? DCP_MINB_P(kernel, L, i, true) : DCP_MINB_P(kernel, L, i, false))
 // Dense or paged variant of a kernel template whose last parameter selects it.
 #define DCP_PAGED(kernel, ...) (B.pool_cap > 0 ? kernel<__VA_ARGS__, true> : kernel<__VA_ARGS__, false>)

@@ -98,8 +98,8 @@ typedef struct DcpOptions {
   int32_t grid_ctas;   /* CTAs of the grid-update kernels, 0 = default */
   int32_t scatter_mode; /* 0: warp-aggregated scatter, 1: one atomic per particle and node,
                            2: lane pairs with the same base cell merged by one shuffle */
-  int32_t min_blocks[3]; /* register caps of k_tri_forward, k_g2p_adj, k_tri_adj as resident 256-thread
-                           CTAs per SM (1 = none, 2, 3, 4); 0 = default */
+  int32_t min_blocks[3]; /* register-cap levels of k_tri_forward, k_g2p_adj, k_tri_adj: 1 = none,
+                           2 = 128, 3 = 96, 4 = 80, 5 = 72, 6 = 64 registers; 0 = default */
   int32_t adj_scatter_mode; /* scatter of the adjoint G2P kernel (k_g2p_adj), same values as
                                scatter_mode, which covers the two P2G kernels */
   int32_t pool_blocks;  /* 0: dense grids (every 4^3-node block of every instance's grid in memory).

@@ -47,4 +47,4 @@ def test_committed_cache_entries_are_valid_launch_options():
         kw = autotune.batch_kwargs(ent["config"])
         assert kw["chunk"] % 32 == 0 and 32 <= kw["chunk"] <= 256
         assert kw["scatter_mode"] in (0, 1, 2) and kw["adj_scatter_mode"] in (0, 1, 2)
-        assert len(kw["min_blocks"]) == 3 and all(1 <= v <= 4 for v in kw["min_blocks"])
+        assert len(kw["min_blocks"]) == 3 and all(1 <= v <= 6 for v in kw["min_blocks"])

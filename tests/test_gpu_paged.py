@@ -60,7 +60,7 @@ def _agree(paged, dense):
 
 @pytest.mark.parametrize("tape", ["auto", None])
 @pytest.mark.parametrize("launch", [dict(scatter_mode=0, adj_scatter_mode=0),
-                                    dict(scatter_mode=2, adj_scatter_mode=2, chunk=64, min_blocks=(4, 4, 2)),
+                                    dict(scatter_mode=2, adj_scatter_mode=2, chunk=64, min_blocks=(6, 5, 3)),
                                     dict(scatter_mode=1, adj_scatter_mode=1, min_blocks=(3, 3, 3))])
 def test_paged_sheets_match_dense_grids(tape, launch):
     scenes = _sheets()
