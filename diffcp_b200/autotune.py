@@ -2,7 +2,7 @@
 
 Chooses, by timing a few eager forward and adjoint substeps of the actual
 workload on the device:
-  * ``chunk``        particles per CTA (64, 128, 256),
+  * ``chunk``        particles per CTA (32, 64, 128, 256),
   * ``scatter_mode`` warp-aggregated runs (0), one atomic per particle and
                      node (1), or lane pairs sharing a base cell (2), for
                      the two P2G kernels, and ``adj_scatter_mode`` likewise
@@ -89,7 +89,7 @@ def tune(scenes: Sequence[ClothScene], dt: float, substeps: int = 3, device=None
             return table[key]["config"]
     modes = (0, 1, 2)
     runs = []
-    for chunk in (64, 128, 256):
+    for chunk in (32, 64, 128, 256):
         per_mode = {}
         for mode in modes:
             # the same mode for P2G and the adjoint: the two scatters are timed
