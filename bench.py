@@ -153,6 +153,33 @@ def ncu_traffic(kernel):
     return ncu_figure(kernel, "dram_bytes_per_launch")
 
 
+def step_issue(prof, restored, ms_per_step, sm_mhz):
+    """Warp instructions of one step, from the per-launch counts of the ncu
+    summaries and the eager profile's launch counts, against the SMs' issue
+    ceiling over the step's time.  The P2G kernels' adjoint launches that
+    return at once (the tape holds their substep, ``restored`` of them) are
+    not counted; kernels without a summary are left out and named."""
+    import torch
+    if not sm_mhz:
+        return None
+    inst, counted, missing = 0.0, [], []
+    for name, (ms, launches) in sorted(prof.items()):
+        per = ncu_figure(name, "warp_inst_per_launch")
+        if per is None:
+            missing.append(name)
+            continue
+        full = launches - (restored if name in ("k_tri_forward", "k_point_p2g") else 0)
+        inst += per * max(full, 0)
+        counted.append(name)
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    peak = 4.0 * sms * sm_mhz * 1e6
+    achieved = inst / (ms_per_step / 1e3)
+    share = sum(prof[k][0] for k in counted) / max(sum(v[0] for v in prof.values()), 1e-12)
+    return {"achieved": achieved, "peak": peak, "unit": "warp instructions/s", "frac": achieved / peak,
+            "warp_inst_per_step": inst, "kernels": counted, "not_counted": missing,
+            "profile_share_counted": share}
+
+
 def issue_ceiling(kernel, avg_launch_s, sm_mhz):
     """The kernel's instruction-issue rate against the SMs' issue ceiling (one
     warp instruction per cycle on each of an SM's 4 schedulers) at the SM
@@ -492,6 +519,8 @@ def main():
                 "peak_device_bytes": int(torch.cuda.max_memory_allocated(dev))},
         "roofline": roof,
         "issue_roofline": issue_ceiling(dname, dms / dn / 1e3, clocks.get("sm_mhz")),
+        "step_issue_roofline": step_issue(prof, tape_info["substeps_restored"] if tape_info else 0, ms_max,
+                                          clocks.get("sm_mhz")),
         "step_roofline": {"achieved": step_alg / (ms_max / 1e3) / 1e9, "unit": "GB/s", "peak": peak,
                           "frac": step_alg / (ms_max / 1e3) / 1e9 / peak,
                           "bytes_per_particle": STEP_BYTES},

@@ -39,3 +39,24 @@ def test_summary_carries_the_figures_bench_reads(kernel):
     assert m and 1.9 / c < traffic / (float(m.group(1)) * 1e6) < 2.1 / c, kernel
     w = re.search(r"\| warp instructions \| ([0-9,]+)", text)
     assert w and 1.9 / c < inst / float(w.group(1).replace(",", "")) < 2.1 / c, kernel
+
+
+def test_step_issue_counts_full_launches_only(monkeypatch):
+    """The whole-step issue figure: per-launch instruction counts times full
+    launches (the P2G kernels' early-exit adjoint launches left out) over the
+    step time, against 4 warp instructions per cycle per SM."""
+    import torch
+
+    class Props:
+        multi_processor_count = 148
+
+    monkeypatch.setattr(torch.cuda, "get_device_properties", lambda i: Props())
+    prof = {"k_tri_forward": (78.4, 600), "k_g2p_adj": (99.6, 300), "k_unprofiled": (1.0, 300)}
+    r = bench.step_issue(prof, 300, 400.0, 2000.0)
+    inst = 300 * bench.ncu_figure("k_tri_forward", "warp_inst_per_launch") + \
+        300 * bench.ncu_figure("k_g2p_adj", "warp_inst_per_launch")
+    assert r["warp_inst_per_step"] == pytest.approx(inst)
+    assert r["peak"] == pytest.approx(4 * 148 * 2000e6)
+    assert r["frac"] == pytest.approx(inst / 0.4 / r["peak"])
+    assert r["not_counted"] == ["k_unprofiled"] and r["profile_share_counted"] == pytest.approx(178.0 / 179.0)
+    assert bench.step_issue(prof, 300, 400.0, None) is None
