@@ -900,22 +900,27 @@ __global__ void __maxnreg__(REGS) k_g2p_adj(BatchDev B, const float* __restrict_
         float kij[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) kij[a] = add_off(add_off(Kg[a], oi, cbC[3 * a]), oj, cbC[3 * a + 1]);
+        // sum factorisation over the column's z nodes, as in k_tri_adj
+        float Rw[3] = {0.f, 0.f, 0.f}, Sw = 0.f, Se = 0.f;
 #pragma unroll
         for (int ok = 0; ok < 3; ++ok) {
           const float w2 = st.w[2][ok];
-          const float W = w01 * w2;
-          const float gW[3] = {e0w1 * w2, w0e1 * w2, w01 * ed[2][ok]};
           const float3 gn = gv_at(gnb, nofs, oi, oj, ok);
           const float ga[3] = {gn.x, gn.y, gn.z};
           float s1 = 0.f;
 #pragma unroll
-          for (int a = 0; a < 3; ++a) s1 += ga[a] * add_off(kij[a], ok, cbC[3 * a + 2]);
-#pragma unroll
-          for (int b = 0; b < 3; ++b) {
-            px[b] += s1 * gW[b];
-            vs[b] += W * ga[b];
+          for (int a = 0; a < 3; ++a) {
+            s1 += ga[a] * add_off(kij[a], ok, cbC[3 * a + 2]);
+            Rw[a] += w2 * ga[a];
           }
+          Sw += w2 * s1;
+          Se += ed[2][ok] * s1;
         }
+        px[0] += e0w1 * Sw;
+        px[1] += w0e1 * Sw;
+        px[2] += w01 * Se;
+#pragma unroll
+        for (int b = 0; b < 3; ++b) vs[b] += w01 * Rw[b];
       }
     // - c4 inv_dx sum_nodes W bC^T g = - inv_dx cbC^T (sum_nodes W g)
 #pragma unroll
@@ -1089,6 +1094,7 @@ __global__ void __launch_bounds__(256, 4) k_point_adj(BatchDev B, const float* _
   float px[3] = {0.f, 0.f, 0.f};
   const float4* gnb = grid_base<PAGED>(B.grid_adj, I);
   const StenAddr<PAGED> nofs(B, I, st.base, true, ch.inst);
+  // sum factorisation over each (oi, oj) column's z nodes, as in k_tri_adj
 #pragma unroll
   for (int oi = 0; oi < 3; ++oi)
 #pragma unroll
@@ -1098,26 +1104,34 @@ __global__ void __launch_bounds__(256, 4) k_point_adj(BatchDev B, const float* _
       float kij[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) kij[a] = add_off(add_off(K[a], oi, Cd[3 * a]), oj, Cd[3 * a + 1]);
+      float Rw[3] = {0.f, 0.f, 0.f}, Rk[3] = {0.f, 0.f, 0.f}, Sw = 0.f, Se = 0.f;
 #pragma unroll
       for (int ok = 0; ok < 3; ++ok) {
         const float w2 = st.w[2][ok];
-        const float W = w01 * w2;
-        const float gW[3] = {e0w1 * w2, w0e1 * w2, w01 * ed[2][ok]};
         const float4 g = __ldg(gnb + nofs.at(oi, oj, ok));
         const float bp[3] = {g.x, g.y, g.z};
         float s = g.w * m;
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
           s += bp[a] * add_off(kij[a], ok, Cd[3 * a + 2]);
-          const float Wb = W * bp[a];
-          sp[a] += Wb;
-          mo[3 * a] = add_off(mo[3 * a], oi, Wb);
-          mo[3 * a + 1] = add_off(mo[3 * a + 1], oj, Wb);
-          mo[3 * a + 2] = add_off(mo[3 * a + 2], ok, Wb);
+          const float wb = w2 * bp[a];
+          Rw[a] += wb;
+          Rk[a] = add_off(Rk[a], ok, wb);
         }
-#pragma unroll
-        for (int b = 0; b < 3; ++b) px[b] += s * gW[b];
+        Sw += w2 * s;
+        Se += ed[2][ok] * s;
       }
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const float Wb = w01 * Rw[a];
+        sp[a] += Wb;
+        mo[3 * a] = add_off(mo[3 * a], oi, Wb);
+        mo[3 * a + 1] = add_off(mo[3 * a + 1], oj, Wb);
+        mo[3 * a + 2] += w01 * Rk[a];
+      }
+      px[0] += e0w1 * Sw;
+      px[1] += w0e1 * Sw;
+      px[2] += w01 * Se;
     }
   float spd[9];  // sum W bp (x) dpos
 #pragma unroll
@@ -1232,6 +1246,11 @@ __global__ void __maxnreg__(REGS) k_tri_adj(BatchDev B, const float* __restrict_
     float hs[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // (00, 01, 02, 11, 12, 22)
     const float4* gnb = grid_base<PAGED>(B.grid_adj, I);
     const StenAddr<PAGED> nofs(B, I, st.base, true, ch.inst);
+    // Sum factorisation: every node weight is a product of per-axis factors,
+    // so the sums over the stencil's z column (ok) are formed first, per
+    // (oi, oj), and scaled by the (x, y) factors once per column:
+    //   Rw[a] = sum_k w2 bp_a, Rk[a] = sum_k o_k w2 bp_a, Re[a] = sum_k e2 bp_a
+    //   Tw, Te, Td = sum_k (w2, e2, dd2) (bp . P3), Sw, Se = sum_k (w2, e2) s
 #pragma unroll
     for (int oi = 0; oi < 3; ++oi)
 #pragma unroll
@@ -1242,33 +1261,51 @@ __global__ void __maxnreg__(REGS) k_tri_adj(BatchDev B, const float* __restrict_
         float kij[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) kij[a] = add_off(add_off(K[a], oi, Cm[3 * a]), oj, Cm[3 * a + 1]);
+        float Rw[3] = {0.f, 0.f, 0.f}, Rk[3] = {0.f, 0.f, 0.f}, Re[3] = {0.f, 0.f, 0.f};
+        float Tw = 0.f, Te = 0.f, Td = 0.f, Sw = 0.f, Se = 0.f;
 #pragma unroll
         for (int ok = 0; ok < 3; ++ok) {
           const float w2 = st.w[2][ok], e2 = ed[2][ok];
-          const float W = w01 * w2;
-          const float gW[3] = {e0w1 * w2, w0e1 * w2, w01 * e2};
-          const float H[6] = {d0w1 * w2, e0e1 * w2, e0w1 * e2, w0d1 * w2, w0e1 * e2, w01 * ddc[ok]};
           const float4 ga = __ldg(gnb + nofs.at(oi, oj, ok));
           const float bp[3] = {ga.x, ga.y, ga.z};
-          const float gdot = gW[0] * d3[0] + gW[1] * d3[1] + gW[2] * d3[2];
           const float sP = bp[0] * P3[0] + bp[1] * P3[1] + bp[2] * P3[2];
-          float s = ga.w * m;
+          float sn = ga.w * m;
 #pragma unroll
           for (int a = 0; a < 3; ++a) {
-            s += bp[a] * add_off(kij[a], ok, Cm[3 * a + 2]);
-            const float Wb = W * bp[a];
-            sp[a] += Wb;
-            mo[3 * a] = add_off(mo[3 * a], oi, Wb);
-            mo[3 * a + 1] = add_off(mo[3 * a + 1], oj, Wb);
-            mo[3 * a + 2] = add_off(mo[3 * a + 2], ok, Wb);
-            g3[a] += gdot * bp[a];
-            sg[a] += sP * gW[a];
+            sn += bp[a] * add_off(kij[a], ok, Cm[3 * a + 2]);
+            const float wb = w2 * bp[a];
+            Rw[a] += wb;
+            Rk[a] = add_off(Rk[a], ok, wb);
+            Re[a] += e2 * bp[a];
           }
-#pragma unroll
-          for (int b = 0; b < 3; ++b) bx[b] += s * gW[b];
-#pragma unroll
-          for (int q = 0; q < 6; ++q) hs[q] += sP * H[q];
+          Tw += w2 * sP;
+          Te += e2 * sP;
+          Td += ddc[ok] * sP;
+          Sw += w2 * sn;
+          Se += e2 * sn;
         }
+        const float c1 = d3[0] * e0w1 + d3[1] * w0e1, c2 = d3[2] * w01;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const float Wb = w01 * Rw[a];
+          sp[a] += Wb;
+          mo[3 * a] = add_off(mo[3 * a], oi, Wb);
+          mo[3 * a + 1] = add_off(mo[3 * a + 1], oj, Wb);
+          mo[3 * a + 2] += w01 * Rk[a];
+          g3[a] += c1 * Rw[a] + c2 * Re[a];
+        }
+        sg[0] += e0w1 * Tw;
+        sg[1] += w0e1 * Tw;
+        sg[2] += w01 * Te;
+        hs[0] += d0w1 * Tw;
+        hs[1] += e0e1 * Tw;
+        hs[2] += e0w1 * Te;
+        hs[3] += w0d1 * Tw;
+        hs[4] += w0e1 * Te;
+        hs[5] += w01 * Td;
+        bx[0] += e0w1 * Sw;
+        bx[1] += w0e1 * Sw;
+        bx[2] += w01 * Se;
       }
     float spd[9], bP3[3], bd3[3];
 #pragma unroll
